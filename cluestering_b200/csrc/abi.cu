@@ -1,0 +1,815 @@
+// abi.cu — the extern "C" entry points of libclue_sm100.so (include/clue_sm100.h):
+// parameter validation, workspace management, host/device clustering calls and
+// result accessors. The serving loop lives in server.cu.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "abi_internal.h"
+
+using namespace clue_impl;
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+
+namespace {
+thread_local std::string t_last_error;
+}
+
+namespace clue_impl {
+
+clue_status fail(clue_status s, const std::string& msg) {
+  t_last_error = msg;
+  return s;
+}
+
+clue_status fail_cuda(cudaError_t e, const char* where) {
+  return fail(e == cudaErrorMemoryAllocation ? CLUE_ERR_OUT_OF_MEMORY : CLUE_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Tables
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr int kChunkPoints = 4096;
+
+// core/detail/SetupTiles.hpp:30-34.
+bool grid_shape(int D, int64_t n, int ppt, int32_t* k_out, int64_t* T_out) {
+  const int64_t nt = (n + ppt - 1) / ppt;
+  int64_t k = 1;
+  auto powk = [D](int64_t k) {
+    int64_t p = 1;
+    for (int d = 0; d < D; ++d) {
+      p *= k;
+      if (p > (int64_t)1 << 40)
+        return p;
+    }
+    return p;
+  };
+  while (powk(k) < nt)
+    ++k;
+  *k_out = (int32_t)k;
+  *T_out = powk(k);
+  return *T_out < INT32_MAX;
+}
+
+void fill_grid(GridDesc* g, int D, int32_t k, int64_t T) {
+  std::memset(g, 0, sizeof(GridDesc));
+  g->k = k;
+  g->T = (int32_t)T;
+  int32_t s = 1;
+  for (int d = D - 1; d >= 0; --d) {
+    g->stride[d] = s;
+    s *= k;
+  }
+}
+}  // namespace
+
+bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode, int32_t ppt,
+                  HostTables* t, RunShape* sh, const char** err) {
+  ppt = ppt > 0 ? ppt : 128;
+  int64_t N = 0;
+  for (int e = 0; e < B; ++e)
+    N += sizes[e];
+  if (N <= 0 || N >= INT32_MAX) {
+    *err = N <= 0 ? "the number of points must be positive" : "too many points for int32 indices";
+    return false;
+  }
+  t->grids.clear();
+  t->events.clear();
+  t->chunks.clear();
+  t->events.resize(B);
+  int64_t tiles = 0;
+  int64_t begin = 0;
+  if (grid_mode == CLUE_GRID_SHARED) {
+    int32_t k;
+    int64_t T;
+    if (!grid_shape(D, N, ppt, &k, &T) || T * B >= INT32_MAX) {
+      *err = "tile grid too large";
+      return false;
+    }
+    t->grids.resize(1);
+    fill_grid(&t->grids[0], D, k, T);
+    for (int e = 0; e < B; ++e) {
+      t->events[e] = EventDesc{(int32_t)begin, (int32_t)sizes[e], (int32_t)(T * e), 0};
+      begin += sizes[e];
+    }
+    tiles = T * B;
+  } else {
+    t->grids.resize(B);
+    for (int e = 0; e < B; ++e) {
+      int32_t k;
+      int64_t T;
+      if (!grid_shape(D, sizes[e], ppt, &k, &T)) {
+        *err = "tile grid too large";
+        return false;
+      }
+      fill_grid(&t->grids[e], D, k, T);
+      t->events[e] = EventDesc{(int32_t)begin, (int32_t)sizes[e], (int32_t)tiles, e};
+      begin += sizes[e];
+      tiles += T;
+      if (tiles >= INT32_MAX) {
+        *err = "tile grid too large";
+        return false;
+      }
+    }
+  }
+  for (int e = 0; e < B; ++e) {
+    const EventDesc& ev = t->events[e];
+    for (int32_t c = ev.begin; c < ev.begin + ev.n; c += kChunkPoints)
+      t->chunks.push_back(Chunk{e, c, std::min(ev.begin + ev.n, c + kChunkPoints)});
+  }
+  sh->D = D;
+  sh->n = N;
+  sh->n_tiles = tiles;
+  sh->n_events = B;
+  sh->n_grids = (int32_t)t->grids.size();
+  sh->n_chunks = (int32_t)t->chunks.size();
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Workspace memory
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct Layout {
+  size_t total = 0;
+  template <typename T>
+  size_t add(int64_t count) {
+    const size_t off = total;
+    total += ((size_t)std::max<int64_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
+    return off;
+  }
+};
+
+// Places every buffer of `cap` in one allocation (or measures it when base is null).
+size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
+  Layout L;
+  const int64_t N = c.points, T = c.tiles, D = c.dims;
+  auto at = [&](size_t off) { return base ? base + off : nullptr; };
+#define CLUE_PLACE(field, type, count) \
+  do {                                 \
+    size_t o_ = L.add<type>(count);    \
+    b->field = (type*)at(o_);          \
+  } while (0)
+  CLUE_PLACE(grids, GridDesc, c.grids);
+  CLUE_PLACE(events, EventDesc, c.events);
+  CLUE_PLACE(chunks, Chunk, c.chunks);
+  CLUE_PLACE(grid_minmax, int32_t, c.grids * 2 * kMaxDim);
+  CLUE_PLACE(tile_of, int32_t, N);
+  CLUE_PLACE(point_event, int32_t, N);
+  CLUE_PLACE(nh, int32_t, N);
+  CLUE_PLACE(seed_flag, int32_t, N);
+  CLUE_PLACE(seed_rank, int32_t, N);
+  CLUE_PLACE(parent, int32_t, N);
+  CLUE_PLACE(tile_count, int32_t, T);
+  CLUE_PLACE(tile_offset, int32_t, T + 1);
+  CLUE_PLACE(tile_cursor, int32_t, T);
+  CLUE_PLACE(perm, int32_t, N);
+  CLUE_PLACE(sorted_event, int32_t, N);
+  CLUE_PLACE(sorted_coords, float, D * N);
+  CLUE_PLACE(sorted_weight, float, N);
+  CLUE_PLACE(sorted_rho, float, N);
+  CLUE_PLACE(merge_tmp, int32_t, N);
+  CLUE_PLACE(seeds, int32_t, N);
+  CLUE_PLACE(seed_event, int32_t, N);
+  CLUE_PLACE(scan_desc, unsigned long long, c.scan_blocks);
+  CLUE_PLACE(counters, int32_t, 16);
+  CLUE_PLACE(oversize, int32_t, N / 4096 + 1);
+  CLUE_PLACE(status, uint32_t, 1);
+  CLUE_PLACE(sorted_sigma, float, c.sigma ? D * N : 0);
+  CLUE_PLACE(sorted_unc, float, c.unc ? N : 0);
+  CLUE_PLACE(sorted_tag, uint32_t, c.tags ? N : 0);
+  const int64_t S = c.staged_points;
+  CLUE_PLACE(in_coords, float, S ? D * S : 0);
+  CLUE_PLACE(in_weight, float, S);
+  CLUE_PLACE(in_sigma, float, (S && c.sigma) ? D * S : 0);
+  CLUE_PLACE(in_unc, float, (S && c.unc) ? S : 0);
+  CLUE_PLACE(in_tags, uint32_t, (S && c.tags) ? S : 0);
+  CLUE_PLACE(out_cluster, int32_t, S);
+  CLUE_PLACE(out_seed, int32_t, S);
+  CLUE_PLACE(out_rho, float, S);
+  CLUE_PLACE(out_nh, int32_t, S);
+#undef CLUE_PLACE
+  return L.total;
+}
+
+}  // namespace
+
+size_t scratch_bytes(const RunShape& s, bool sigma, bool unc, bool tags) {
+  Capacity c;
+  c.points = s.n;
+  c.tiles = s.n_tiles;
+  c.events = s.n_events;
+  c.chunks = s.n_chunks;
+  c.grids = s.n_grids;
+  c.scan_blocks = scan_blocks_for(std::max<int64_t>(s.n, s.n_tiles));
+  c.dims = s.D;
+  c.sigma = sigma;
+  c.unc = unc;
+  c.tags = tags;
+  DeviceBuffers b;
+  return place(&b, c, nullptr);
+}
+
+clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, bool unc, bool tags,
+                            int64_t staged) {
+  Capacity& c = ws->cap;
+  const int64_t scan_blocks = scan_blocks_for(std::max<int64_t>(s.n, s.n_tiles));
+  const bool fits = c.points >= s.n && c.tiles >= s.n_tiles && c.events >= s.n_events &&
+                    c.chunks >= s.n_chunks && c.grids >= s.n_grids &&
+                    c.scan_blocks >= scan_blocks && c.dims >= s.D && (!sigma || c.sigma) &&
+                    (!unc || c.unc) && (!tags || c.tags) && c.staged_points >= staged;
+  if (fits)
+    return CLUE_OK;
+  // Grow every dimension that is short by 25 % headroom; keep what fits.
+  auto grow = [](int64_t have, int64_t need) { return have >= need ? have : need + need / 4; };
+  Capacity n = c;
+  n.points = grow(c.points, s.n);
+  n.tiles = grow(c.tiles, s.n_tiles);
+  n.events = grow(c.events, s.n_events);
+  n.chunks = grow(c.chunks, s.n_chunks);
+  n.grids = grow(c.grids, s.n_grids);
+  n.scan_blocks = scan_blocks_for(std::max<int64_t>(n.points, n.tiles));
+  n.dims = std::max(c.dims, s.D);
+  n.sigma = c.sigma || sigma;
+  n.unc = c.unc || unc;
+  n.tags = c.tags || tags;
+  n.staged_points = staged ? grow(c.staged_points, staged) : c.staged_points;
+  DeviceBuffers nb;
+  const size_t bytes = place(&nb, n, nullptr);
+  if (ws->base) {
+    // cudaFree waits for the device; earlier runs on any stream are finished.
+    cudaFree(ws->base);
+    ws->base = nullptr;
+    ws->bytes = 0;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    ws->cap = Capacity{};
+    ws->b = DeviceBuffers{};
+    return fail_cuda(e, "workspace allocation");
+  }
+  ws->base = (char*)p;
+  ws->bytes = bytes;
+  place(&ws->b, n, ws->base);
+  ws->cap = n;
+  cudaMemset(ws->b.status, 0, sizeof(uint32_t));
+  return CLUE_OK;
+}
+
+clue_status check_params(const clue_params* p) {
+  if (!p)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "params is null");
+  // core/detail/Clusterer.hpp:42-48
+  if (!(p->dc > 0.0f) || !(p->rhoc >= 0.0f) || !(p->dm > 0.0f) || !(p->seed_dc > 0.0f))
+    return fail(CLUE_ERR_INVALID_ARGUMENT,
+                "Invalid clustering parameters. The parameters must be positive.");
+  // core/detail/ConvolutionalKernel.hpp:13-50
+  switch (p->kernel_kind) {
+    case CLUE_KERNEL_FLAT:
+      if (!(p->kernel_params[0] > 0.0f))
+        return fail(CLUE_ERR_INVALID_ARGUMENT, "Flat kernel parameter must be positive.");
+      break;
+    case CLUE_KERNEL_GAUSSIAN:
+      if (!(p->kernel_params[0] > 0.0f) || !(p->kernel_params[1] > 0.0f))
+        return fail(CLUE_ERR_INVALID_ARGUMENT, "Gaussian kernel parameters must be positive.");
+      break;
+    case CLUE_KERNEL_EXPONENTIAL:
+      if (!(p->kernel_params[0] > 0.0f) || !(p->kernel_params[1] > 0.0f))
+        return fail(CLUE_ERR_INVALID_ARGUMENT, "Exponential kernel parameters must be positive.");
+      break;
+    default:
+      return fail(CLUE_ERR_INVALID_ARGUMENT, "unknown convolutional kernel");
+  }
+  if (p->metric_kind < CLUE_METRIC_EUCLIDEAN || p->metric_kind > CLUE_METRIC_MAHALANOBIS)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "unknown distance metric");
+  if (p->points_per_tile < 0)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "points_per_tile must be >= 0");
+  return CLUE_OK;
+}
+
+clue_status check_points(const clue_points* pts, bool need_output, int metric_kind) {
+  if (!pts)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "points is null");
+  if (pts->ndim < 1 || pts->ndim > CLUE_MAX_DIM)
+    return fail(CLUE_ERR_OUT_OF_RANGE, "ndim must be in [1, 10]");
+  if (pts->n <= 0)
+    return fail(CLUE_ERR_INVALID_ARGUMENT,
+                "Number of points passed to the points constructor must be positive.");
+  for (int d = 0; d < pts->ndim; ++d)
+    if (!pts->coords[d])
+      return fail(CLUE_ERR_INVALID_ARGUMENT, "missing coordinate array");
+  if (!pts->weight)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "missing weight array");
+  if (need_output && !pts->cluster_index)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "missing cluster_index output");
+  if (metric_kind == CLUE_METRIC_MAHALANOBIS)
+    for (int d = 0; d < pts->ndim; ++d)
+      if (!pts->sigma[d])
+        return fail(CLUE_ERR_INVALID_ARGUMENT,
+                    "the Mahalanobis metric needs sigma for every dimension");
+  return CLUE_OK;
+}
+
+// Largest float x >= 0 with sqrtf(x) <= r (sqrt is correctly rounded on host
+// and device, and monotone, so `sqrt(d2) <= r` is exactly `d2 <= x`).
+float sqrt_threshold(float r) {
+  if (!(r >= 0.0f))
+    return -1.0f;
+  if (std::isinf(r))
+    return INFINITY;
+  float x = (float)((double)r * (double)r);
+  if (!std::isfinite(x))
+    x = FLT_MAX;
+  while (x > 0.0f && std::sqrt(x) > r)
+    x = std::nextafter(x, 0.0f);
+  for (;;) {
+    const float up = std::nextafter(x, INFINITY);
+    if (std::isinf(up) || std::sqrt(up) > r)
+      break;
+    x = up;
+  }
+  return x;
+}
+
+RunParams make_run_params(const clue_params* p, const clue_points* pts) {
+  RunParams r{};
+  r.D = pts->ndim;
+  r.dc = p->dc;
+  r.rhoc = p->rhoc;
+  r.dm = p->dm;
+  r.seed_dc = p->seed_dc;
+  for (int d = 0; d < kMaxDim; ++d) {
+    r.wrapped[d] = p->wrapped[d] ? 1 : 0;
+    r.mparam[d] = p->metric_params[d];
+  }
+  r.kernel_kind = p->kernel_kind;
+  r.kernel_p0 = p->kernel_params[0];
+  r.kernel_p1 = p->kernel_params[1];
+  r.metric_kind = p->metric_kind;
+  r.dc2 = sqrt_threshold(p->dc);
+  r.dm2 = sqrt_threshold(p->dm);
+  r.seed2 = sqrt_threshold(p->seed_dc);
+  r.has_sigma = 0;
+  for (int d = 0; d < pts->ndim; ++d)
+    if (pts->sigma[d])
+      r.has_sigma |= 1 << d;
+  r.has_unc = pts->density_uncertainty != nullptr;
+  r.has_tags = pts->tags != nullptr;
+  return r;
+}
+
+// Uploads the host tables through the workspace's pinned staging buffer.
+clue_status upload_tables(clue_workspace* ws, const HostTables& t, cudaStream_t st) {
+  const size_t g = t.grids.size() * sizeof(GridDesc);
+  const size_t e = t.events.size() * sizeof(EventDesc);
+  const size_t c = t.chunks.size() * sizeof(Chunk);
+  const size_t need = g + e + c;
+  // The previous upload must have left the staging buffer before it is reused.
+  if (ws->staging_event)
+    cudaEventSynchronize(ws->staging_event);
+  if (ws->staging_bytes < need) {
+    if (ws->staging)
+      cudaFreeHost(ws->staging);
+    ws->staging = nullptr;
+    ws->staging_bytes = 0;
+    cudaError_t err = cudaMallocHost(&ws->staging, need + need / 4);
+    if (err != cudaSuccess)
+      return fail_cuda(err, "pinned staging allocation");
+    ws->staging_bytes = need + need / 4;
+  }
+  char* h = (char*)ws->staging;
+  std::memcpy(h, t.grids.data(), g);
+  std::memcpy(h + g, t.events.data(), e);
+  std::memcpy(h + g + e, t.chunks.data(), c);
+  cudaError_t err;
+  if ((err = cudaMemcpyAsync(ws->b.grids, h, g, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (err = cudaMemcpyAsync(ws->b.events, h + g, e, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (err = cudaMemcpyAsync(ws->b.chunks, h + g + e, c, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return fail_cuda(err, "table upload");
+  cudaEventRecord(ws->staging_event, st);
+  return CLUE_OK;
+}
+
+// One run on device-resident points. `sizes` is the host event table.
+clue_status run_device(clue_workspace* ws, const clue_params* params, const clue_points* pts,
+                       const uint32_t* sizes, int32_t n_events, int32_t grid_mode,
+                       cudaStream_t st, int64_t staged) {
+  clue_status s = check_params(params);
+  if (s != CLUE_OK)
+    return s;
+  if ((s = check_points(pts, true, params->metric_kind)) != CLUE_OK)
+    return s;
+  cudaError_t e = cudaSetDevice(ws->device);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "cudaSetDevice");
+  HostTables t;
+  RunShape sh;
+  const char* err = nullptr;
+  if (!build_tables(pts->ndim, sizes, n_events, grid_mode, params->points_per_tile, &t, &sh, &err))
+    return fail(CLUE_ERR_INVALID_ARGUMENT, err);
+  if (sh.n != pts->n)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "the event sizes do not add up to the number of points");
+  bool any_sigma = false;
+  for (int d = 0; d < pts->ndim; ++d)
+    any_sigma |= pts->sigma[d] != nullptr;
+  if ((s = ensure_capacity(ws, sh, any_sigma, pts->density_uncertainty != nullptr,
+                           pts->tags != nullptr, staged)) != CLUE_OK)
+    return s;
+  if ((s = upload_tables(ws, t, st)) != CLUE_OK)
+    return s;
+  RunIO io;
+  for (int d = 0; d < pts->ndim; ++d) {
+    io.coords[d] = pts->coords[d];
+    io.sigma[d] = pts->sigma[d];
+  }
+  io.weight = pts->weight;
+  io.unc = pts->density_uncertainty;
+  io.tags = pts->tags;
+  io.cluster_index = pts->cluster_index;
+  io.is_seed = pts->is_seed;
+  io.rho = pts->rho;
+  io.nh = pts->nearest_higher;
+  const RunParams prm = make_run_params(params, pts);
+  if ((e = launch_run(sh, prm, io, ws->b, st)) != cudaSuccess)
+    return fail_cuda(e, "kernel launch");
+  // Seed count and status word come back with the run (read when needed).
+  cudaMemcpyAsync(&ws->info->n_seeds, ws->b.counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                  st);
+  cudaMemcpyAsync(&ws->info->status, ws->b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  cudaEventRecord(ws->run_event, st);
+  ws->has_run = true;
+  ws->last_n = sh.n;
+  ws->last_events = t.events;
+  return CLUE_OK;
+}
+
+clue_status wait_run(clue_workspace* ws) {
+  if (!ws->has_run)
+    return fail(CLUE_ERR_RUNTIME, "Seeds are not available. Please run make_clusters first.");
+  cudaError_t e = cudaEventSynchronize(ws->run_event);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "run");
+  if (ws->info->status != 0)
+    return fail(CLUE_ERR_TIMEOUT, "a bounded device-side wait gave up (status " +
+                                      std::to_string(ws->info->status) + ")");
+  return CLUE_OK;
+}
+
+// Copies one host point set into the workspace's staging buffers and points
+// `dev` at them.
+clue_status stage_inputs(clue_workspace* ws, const clue_points* h, clue_points* dev,
+                         cudaStream_t st) {
+  const int64_t n = h->n;
+  const int D = h->ndim;
+  *dev = *h;
+  cudaError_t e;
+  for (int d = 0; d < D; ++d) {
+    float* dst = ws->b.in_coords + d * n;
+    if ((e = cudaMemcpyAsync(dst, h->coords[d], n * sizeof(float), cudaMemcpyHostToDevice, st)))
+      return fail_cuda(e, "coordinate upload");
+    dev->coords[d] = dst;
+    if (h->sigma[d]) {
+      float* sd = ws->b.in_sigma + d * n;
+      if ((e = cudaMemcpyAsync(sd, h->sigma[d], n * sizeof(float), cudaMemcpyHostToDevice, st)))
+        return fail_cuda(e, "sigma upload");
+      dev->sigma[d] = sd;
+    }
+  }
+  if ((e = cudaMemcpyAsync(ws->b.in_weight, h->weight, n * sizeof(float), cudaMemcpyHostToDevice,
+                           st)))
+    return fail_cuda(e, "weight upload");
+  dev->weight = ws->b.in_weight;
+  if (h->density_uncertainty) {
+    if ((e = cudaMemcpyAsync(ws->b.in_unc, h->density_uncertainty, n * sizeof(float),
+                             cudaMemcpyHostToDevice, st)))
+      return fail_cuda(e, "uncertainty upload");
+    dev->density_uncertainty = ws->b.in_unc;
+  }
+  if (h->tags) {
+    if ((e = cudaMemcpyAsync(ws->b.in_tags, h->tags, n * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             st)))
+      return fail_cuda(e, "tag upload");
+    dev->tags = ws->b.in_tags;
+  }
+  dev->cluster_index = ws->b.out_cluster;
+  dev->is_seed = h->is_seed ? ws->b.out_seed : nullptr;
+  dev->rho = h->rho ? ws->b.out_rho : nullptr;
+  dev->nearest_higher = h->nearest_higher ? ws->b.out_nh : nullptr;
+  return CLUE_OK;
+}
+
+clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st) {
+  const size_t n = (size_t)h->n;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(h->cluster_index, ws->b.out_cluster, n * 4, cudaMemcpyDeviceToHost, st)))
+    return fail_cuda(e, "result download");
+  if (h->is_seed && (e = cudaMemcpyAsync(h->is_seed, ws->b.out_seed, n * 4, cudaMemcpyDeviceToHost, st)))
+    return fail_cuda(e, "result download");
+  if (h->rho && (e = cudaMemcpyAsync(h->rho, ws->b.out_rho, n * 4, cudaMemcpyDeviceToHost, st)))
+    return fail_cuda(e, "result download");
+  if (h->nearest_higher &&
+      (e = cudaMemcpyAsync(h->nearest_higher, ws->b.out_nh, n * 4, cudaMemcpyDeviceToHost, st)))
+    return fail_cuda(e, "result download");
+  return CLUE_OK;
+}
+
+clue_status run_host(clue_workspace* ws, const clue_params* params, const clue_points* h,
+                     const uint32_t* sizes, int32_t n_events, int32_t grid_mode, cudaStream_t st) {
+  clue_status s = check_params(params);
+  if (s != CLUE_OK)
+    return s;
+  if ((s = check_points(h, true, params->metric_kind)) != CLUE_OK)
+    return s;
+  // Make sure the staging buffers exist before copying into them.
+  HostTables t;
+  RunShape sh;
+  const char* err = nullptr;
+  if (!build_tables(h->ndim, sizes, n_events, grid_mode, params->points_per_tile, &t, &sh, &err))
+    return fail(CLUE_ERR_INVALID_ARGUMENT, err);
+  if (sh.n != h->n)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "the event sizes do not add up to the number of points");
+  bool any_sigma = false;
+  for (int d = 0; d < h->ndim; ++d)
+    any_sigma |= h->sigma[d] != nullptr;
+  cudaError_t e = cudaSetDevice(ws->device);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "cudaSetDevice");
+  if ((s = ensure_capacity(ws, sh, any_sigma, h->density_uncertainty != nullptr, h->tags != nullptr,
+                           h->n)) != CLUE_OK)
+    return s;
+  clue_points dev;
+  if ((s = stage_inputs(ws, h, &dev, st)) != CLUE_OK)
+    return s;
+  if ((s = run_device(ws, params, &dev, sizes, n_events, grid_mode, st, h->n)) != CLUE_OK)
+    return s;
+  if ((s = fetch_outputs(ws, h, st)) != CLUE_OK)
+    return s;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return fail_cuda(e, "stream synchronize");
+  return wait_run(ws);
+}
+
+}  // namespace clue_impl
+
+// ---------------------------------------------------------------------------
+// extern "C"
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int32_t clue_abi_version(void) { return CLUE_ABI_VERSION; }
+
+const char* clue_status_string(clue_status s) {
+  switch (s) {
+    case CLUE_OK: return "ok";
+    case CLUE_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case CLUE_ERR_OUT_OF_RANGE: return "out of range";
+    case CLUE_ERR_RUNTIME: return "runtime error";
+    case CLUE_ERR_CUDA: return "CUDA error";
+    case CLUE_ERR_OUT_OF_MEMORY: return "out of memory";
+    case CLUE_ERR_TIMEOUT: return "timeout";
+    case CLUE_ERR_NOT_READY: return "not ready";
+  }
+  return "unknown status";
+}
+
+const char* clue_last_error(void) { return t_last_error.c_str(); }
+
+clue_status clue_validate_params(const clue_params* params) { return check_params(params); }
+
+clue_status clue_workspace_create(clue_workspace** out, int32_t device) {
+  if (!out)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null output pointer");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= count)
+    return fail(CLUE_ERR_OUT_OF_RANGE, "device index out of range");
+  if ((e = cudaSetDevice(device)) != cudaSuccess)
+    return fail_cuda(e, "cudaSetDevice");
+  auto* ws = new clue_workspace();
+  ws->device = device;
+  if ((e = cudaEventCreateWithFlags(&ws->run_event, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&ws->staging_event, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaMallocHost((void**)&ws->info, sizeof(RunInfo))) != cudaSuccess) {
+    delete ws;
+    return fail_cuda(e, "workspace creation");
+  }
+  std::memset(ws->info, 0, sizeof(RunInfo));
+  *out = ws;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_destroy(clue_workspace* ws) {
+  if (!ws)
+    return CLUE_OK;
+  cudaSetDevice(ws->device);
+  if (ws->has_run)
+    cudaEventSynchronize(ws->run_event);
+  if (ws->base)
+    cudaFree(ws->base);
+  if (ws->staging)
+    cudaFreeHost(ws->staging);
+  if (ws->info)
+    cudaFreeHost(ws->info);
+  if (ws->run_event)
+    cudaEventDestroy(ws->run_event);
+  if (ws->staging_event)
+    cudaEventDestroy(ws->staging_event);
+  delete ws;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_bytes(const clue_workspace* ws, size_t* bytes) {
+  if (!ws || !bytes)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  *bytes = ws->bytes;
+  return CLUE_OK;
+}
+
+size_t clue_workspace_bytes_for(int32_t ndim, int64_t n_points, int64_t n_tiles, int32_t n_events) {
+  RunShape s;
+  s.D = ndim;
+  s.n = n_points;
+  s.n_tiles = n_tiles;
+  s.n_events = n_events;
+  s.n_grids = n_events;
+  s.n_chunks = (int32_t)(n_events + n_points / kChunkPoints + 1);
+  return scratch_bytes(s, false, false, false);
+}
+
+clue_status clue_make_clusters_device(clue_workspace* ws, const clue_params* params,
+                                      const clue_points* points, void* stream) {
+  if (!ws)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");
+  if (!points || points->n <= 0)
+    return check_points(points, true, params ? params->metric_kind : 0);
+  const uint32_t size = (uint32_t)points->n;
+  return run_device(ws, params, points, &size, 1, CLUE_GRID_PER_EVENT, (cudaStream_t)stream, 0);
+}
+
+clue_status clue_make_clusters_host(clue_workspace* ws, const clue_params* params,
+                                    const clue_points* points, void* stream) {
+  if (!ws)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");
+  if (!points || points->n <= 0)
+    return check_points(points, true, params ? params->metric_kind : 0);
+  const uint32_t size = (uint32_t)points->n;
+  return run_host(ws, params, points, &size, 1, CLUE_GRID_PER_EVENT, (cudaStream_t)stream);
+}
+
+clue_status clue_make_clusters_batched_device(clue_workspace* ws, const clue_params* params,
+                                              const clue_points* points, const uint32_t* sizes,
+                                              int32_t n_events, int32_t grid_mode, void* stream) {
+  if (!ws || !sizes || n_events <= 0)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace, event sizes and n_events are required");
+  if (grid_mode != CLUE_GRID_SHARED && grid_mode != CLUE_GRID_PER_EVENT)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "unknown grid mode");
+  return run_device(ws, params, points, sizes, n_events, grid_mode, (cudaStream_t)stream, 0);
+}
+
+clue_status clue_make_clusters_batched_host(clue_workspace* ws, const clue_params* params,
+                                            const clue_points* points, const uint32_t* sizes,
+                                            int32_t n_events, int32_t grid_mode, void* stream) {
+  if (!ws || !sizes || n_events <= 0)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace, event sizes and n_events are required");
+  if (grid_mode != CLUE_GRID_SHARED && grid_mode != CLUE_GRID_PER_EVENT)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "unknown grid mode");
+  return run_host(ws, params, points, sizes, n_events, grid_mode, (cudaStream_t)stream);
+}
+
+clue_status clue_n_clusters(clue_workspace* ws, int32_t* n_clusters) {
+  if (!ws || !n_clusters)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  clue_status s = wait_run(ws);
+  if (s != CLUE_OK)
+    return s;
+  *n_clusters = ws->info->n_seeds;
+  return CLUE_OK;
+}
+
+clue_status clue_get_seeds(clue_workspace* ws, int32_t* seeds, int32_t capacity, int32_t* n_seeds) {
+  if (!ws)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");
+  clue_status s = wait_run(ws);
+  if (s != CLUE_OK)
+    return s;
+  const int32_t n = ws->info->n_seeds;
+  if (n_seeds)
+    *n_seeds = n;
+  const int32_t m = std::min(n, std::max(capacity, 0));
+  if (m > 0 && seeds) {
+    cudaError_t e = cudaMemcpy(seeds, ws->b.seeds, sizeof(int32_t) * m, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+      return fail_cuda(e, "seed download");
+  }
+  return CLUE_OK;
+}
+
+clue_status clue_sample_associations(clue_workspace* ws, int32_t* offsets, int32_t capacity,
+                                     int32_t* n_keys) {
+  if (!ws)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");
+  clue_status s = wait_run(ws);
+  if (s != CLUE_OK)
+    return s;
+  const int32_t n = ws->info->n_seeds;
+  std::vector<int32_t> ev(std::max(n, 1));
+  if (n > 0) {
+    cudaError_t e = cudaMemcpy(ev.data(), ws->b.seed_event, sizeof(int32_t) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+      return fail_cuda(e, "association download");
+  }
+  const int32_t B = (int32_t)ws->last_events.size();
+  std::vector<int32_t> off(B + 1, 0);
+  for (int32_t k = 0; k < n; ++k)
+    off[ev[k] + 1] += 1;
+  for (int32_t e = 0; e < B; ++e)
+    off[e + 1] += off[e];
+  if (offsets)
+    for (int32_t e = 0; e <= B && e < capacity; ++e)
+      offsets[e] = off[e];
+  // make_associator sizes the map by the largest key + 1
+  // (data_structures/internal/MakeAssociator.hpp:32-43).
+  if (n_keys)
+    *n_keys = n > 0 ? ev[n - 1] + 1 : 0;
+  return CLUE_OK;
+}
+
+clue_status clue_get_clusters_device(clue_workspace* ws, int32_t* offsets, int32_t* points,
+                                     void* stream) {
+  (void)ws;
+  (void)offsets;
+  (void)points;
+  (void)stream;
+  return fail(CLUE_ERR_RUNTIME, "clue_get_clusters_device is not available in this build");
+}
+
+clue_status clue_stream_create(void** stream, int32_t device) {
+  if (!stream)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "cudaSetDevice");
+  cudaStream_t s;
+  if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail_cuda(e, "cudaStreamCreate");
+  *stream = s;
+  return CLUE_OK;
+}
+
+clue_status clue_stream_destroy(void* stream) {
+  cudaError_t e = cudaStreamDestroy((cudaStream_t)stream);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaStreamDestroy");
+}
+
+clue_status clue_stream_synchronize(void* stream) {
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaStreamSynchronize");
+}
+
+clue_status clue_device_malloc(void** ptr, size_t bytes, int32_t device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess)
+    e = cudaMalloc(ptr, bytes);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaMalloc");
+}
+
+clue_status clue_device_free(void* ptr) {
+  cudaError_t e = cudaFree(ptr);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaFree");
+}
+
+clue_status clue_host_malloc_pinned(void** ptr, size_t bytes) {
+  cudaError_t e = cudaMallocHost(ptr, bytes);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaMallocHost");
+}
+
+clue_status clue_host_free_pinned(void* ptr) {
+  cudaError_t e = cudaFreeHost(ptr);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaFreeHost");
+}
+
+clue_status clue_memcpy_async(void* dst, const void* src, size_t bytes, int32_t kind, void* stream) {
+  const cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice
+                           : kind == 1 ? cudaMemcpyDeviceToHost
+                                       : cudaMemcpyDeviceToDevice;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cudaMemcpyAsync");
+}
+
+}  // extern "C"

@@ -1,0 +1,52 @@
+// abi_internal.h — state behind the opaque handles of the C ABI, shared by
+// abi.cu and server.cu.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "clue_sm100.h"
+#include "engine.h"
+
+// Values a run sends back to pinned host memory when it finishes.
+struct RunInfo {
+  int32_t n_seeds;
+  uint32_t status;
+};
+
+struct clue_workspace {
+  int32_t device = 0;
+  char* base = nullptr;  // one device allocation holding every buffer
+  size_t bytes = 0;
+  clue_impl::DeviceBuffers b;
+  clue_impl::Capacity cap;
+  void* staging = nullptr;  // pinned host buffer for the run tables
+  size_t staging_bytes = 0;
+  cudaEvent_t staging_event = nullptr;
+  cudaEvent_t run_event = nullptr;
+  RunInfo* info = nullptr;  // pinned
+  bool has_run = false;
+  int64_t last_n = 0;
+  std::vector<clue_impl::EventDesc> last_events;
+};
+
+namespace clue_impl {
+
+clue_status fail(clue_status s, const std::string& msg);
+clue_status fail_cuda(cudaError_t e, const char* where);
+clue_status check_params(const clue_params* p);
+clue_status check_points(const clue_points* pts, bool need_output, int metric_kind);
+clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, bool unc, bool tags,
+                            int64_t staged);
+clue_status run_device(clue_workspace* ws, const clue_params* params, const clue_points* pts,
+                       const uint32_t* sizes, int32_t n_events, int32_t grid_mode,
+                       cudaStream_t st, int64_t staged);
+clue_status run_host(clue_workspace* ws, const clue_params* params, const clue_points* h,
+                     const uint32_t* sizes, int32_t n_events, int32_t grid_mode, cudaStream_t st);
+clue_status stage_inputs(clue_workspace* ws, const clue_points* h, clue_points* dev,
+                         cudaStream_t st);
+clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st);
+clue_status wait_run(clue_workspace* ws);
+float sqrt_threshold(float r);
+
+}  // namespace clue_impl

@@ -1,0 +1,117 @@
+// engine.h — host-side interface between the C ABI / serving layer and the
+// CUDA kernels of one clustering run.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace clue_impl {
+
+// Device buffers of one workspace. Sizes grow on demand and never shrink.
+struct DeviceBuffers {
+  // tables
+  GridDesc* grids = nullptr;
+  EventDesc* events = nullptr;
+  Chunk* chunks = nullptr;
+  int32_t* grid_minmax = nullptr;  // 2*D ordered ints per grid (min, max)
+  // per point (original order)
+  int32_t* tile_of = nullptr;
+  int32_t* point_event = nullptr;
+  int32_t* nh = nullptr;           // nearest higher when the caller does not want it
+  int32_t* seed_flag = nullptr;
+  int32_t* seed_rank = nullptr;
+  int32_t* parent = nullptr;
+  // per tile
+  int32_t* tile_count = nullptr;
+  int32_t* tile_offset = nullptr;  // T + 1
+  int32_t* tile_cursor = nullptr;
+  // per sorted position
+  int32_t* perm = nullptr;         // sorted position -> original index
+  int32_t* sorted_event = nullptr;
+  float* sorted_coords = nullptr;  // D planes of n
+  float* sorted_weight = nullptr;
+  float* sorted_sigma = nullptr;   // D planes when sigma is set
+  float* sorted_unc = nullptr;
+  uint32_t* sorted_tag = nullptr;
+  float* sorted_rho = nullptr;
+  int32_t* merge_tmp = nullptr;
+  // seeds
+  int32_t* seeds = nullptr;
+  int32_t* seed_event = nullptr;
+  // scan state
+  unsigned long long* scan_desc = nullptr;
+  int32_t* counters = nullptr;     // [0] scan ticket, [1] n_seeds, [2] oversize count, [3] scan total
+  int32_t* oversize = nullptr;     // tiles needing a chunk merge
+  uint32_t* status = nullptr;
+  // staged inputs/outputs for the host entry points
+  float* in_coords = nullptr;
+  float* in_weight = nullptr;
+  float* in_sigma = nullptr;
+  float* in_unc = nullptr;
+  uint32_t* in_tags = nullptr;
+  int32_t* out_cluster = nullptr;
+  int32_t* out_seed = nullptr;
+  float* out_rho = nullptr;
+  int32_t* out_nh = nullptr;
+};
+
+struct Capacity {
+  int64_t points = 0, tiles = 0, events = 0, chunks = 0, grids = 0, scan_blocks = 0;
+  int32_t dims = 0;
+  bool sigma = false, unc = false, tags = false;
+  int64_t staged_points = 0;
+};
+
+struct RunShape {
+  int32_t D = 0;
+  int64_t n = 0;
+  int64_t n_tiles = 0;
+  int32_t n_events = 0;
+  int32_t n_grids = 0;
+  int32_t n_chunks = 0;
+};
+
+// Pointers of one run's inputs and outputs (device memory).
+struct RunIO {
+  const float* coords[kMaxDim] = {};
+  const float* weight = nullptr;
+  const float* sigma[kMaxDim] = {};
+  const float* unc = nullptr;
+  const uint32_t* tags = nullptr;
+  int32_t* cluster_index = nullptr;
+  int32_t* is_seed = nullptr;
+  float* rho = nullptr;
+  int32_t* nh = nullptr;
+};
+
+// Host tables built for a run.
+struct HostTables {
+  std::vector<GridDesc> grids;
+  std::vector<EventDesc> events;
+  std::vector<Chunk> chunks;
+};
+
+// Builds the grid/event/chunk tables from host-side event sizes. Returns false
+// and sets *err when the configuration is out of range.
+bool build_tables(int32_t D, const uint32_t* sizes, int32_t n_events, int32_t grid_mode,
+                  int32_t points_per_tile, HostTables* t, RunShape* shape, const char** err);
+
+// Bytes of device scratch a run of this shape needs.
+size_t scratch_bytes(const RunShape& s, bool sigma, bool unc, bool tags);
+
+// Enqueues the whole run on `stream`. Tables must already be on the device.
+cudaError_t launch_run(const RunShape& shape, const RunParams& prm, const RunIO& io,
+                       const DeviceBuffers& b, cudaStream_t stream);
+
+// Device -> host helpers used after a run.
+cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, int32_t* offsets,
+                                int32_t* points, int32_t n_clusters_upper, cudaStream_t stream);
+
+int scan_blocks_for(int64_t n);
+
+}  // namespace clue_impl

@@ -1,0 +1,586 @@
+// kernels.cu — the CUDA kernels of one clustering run and the launch sequence.
+//
+// Pipeline (all on one stream, no host round trip between stages):
+//   grid extents  : per-grid min/max of the coordinates, tile size (max-min)/k
+//   tile binning  : counting sort of point ids by tile — warp-aggregated
+//                   histogram, single-pass decoupled-look-back scan, warp-
+//                   aggregated scatter, then each tile's ids put in ascending
+//                   order (the order the reference's serial fill produces)
+//   gather        : tile-contiguous SoA copy of coordinates, weights, options
+//   density sweep : rho per point, summed in the reference's exact order
+//   NH sweep      : nearest higher, the reference's comparisons and tie-breaks
+//   seeds/labels  : exclusive scan of the seed flags (seed k = k-th seed in
+//                   index order gets cluster id k), roots by pointer jumping.
+#include <cfloat>
+#include <cuda/atomic>
+
+#include "engine.h"
+#include "sweep.cuh"
+
+namespace clue_impl {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kThreads * kScanItems;  // elements per scan block
+constexpr int kSortCap = 4096;                    // tile sizes sorted in one shared-memory pass
+constexpr int kSpinLimit = 1 << 21;               // bounded waits (~0.2 s) before flagging
+constexpr unsigned kFull = 0xffffffffu;
+
+struct CoordPtrs {
+  const float* p[kMaxDim];
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_reduce(T v, T (*op)(T, T), T* smem) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v = op(v, __shfl_xor_sync(kFull, v, o));
+  if (lane == 0)
+    smem[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < (int)(blockDim.x >> 5)) ? smem[lane] : smem[0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      v = op(v, __shfl_xor_sync(kFull, v, o));
+  }
+  __syncthreads();
+  return v;  // valid in warp 0
+}
+
+__device__ float fmin_op(float a, float b) { return fminf(a, b); }
+__device__ float fmax_op(float a, float b) { return fmaxf(a, b); }
+
+// ---------------------------------------------------------------------------
+// Grid extents: core/detail/ComputeTiles.hpp:16-62, SetupTiles.hpp:19-96
+// ---------------------------------------------------------------------------
+
+__global__ void k_grid_init(int32_t* grid_minmax, int n_grids) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_grids * kMaxDim) {
+    grid_minmax[2 * i] = f2ord(FLT_MAX);       // min starts at numeric_limits::max()
+    grid_minmax[2 * i + 1] = f2ord(-FLT_MAX);  // max starts at numeric_limits::lowest()
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_minmax(int D, CoordPtrs x, const Chunk* chunks,
+                                                     const EventDesc* events, int32_t* grid_minmax) {
+  __shared__ float red[32];
+  const Chunk c = chunks[blockIdx.x];
+  const int g = events[c.event].grid;
+  for (int d = 0; d < D; ++d) {
+    float mn = FLT_MAX, mx = -FLT_MAX;
+    for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
+      const float v = x.p[d][i];
+      if (v == v) {  // NaN never becomes an extreme
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+      }
+    }
+    mn = block_reduce(mn, fmin_op, red);
+    mx = block_reduce(mx, fmax_op, red);
+    if (threadIdx.x == 0) {
+      atomicMin(&grid_minmax[2 * (g * kMaxDim + d)], f2ord(mn));
+      atomicMax(&grid_minmax[2 * (g * kMaxDim + d) + 1], f2ord(mx));
+    }
+  }
+}
+
+__global__ void k_grid_finalize(int D, GridDesc* grids, int n_grids, const int32_t* grid_minmax) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_grids)
+    return;
+  for (int d = 0; d < D; ++d) {
+    const float mn = ord2f(grid_minmax[2 * (g * kMaxDim + d)]);
+    const float mx = ord2f(grid_minmax[2 * (g * kMaxDim + d) + 1]);
+    grids[g].minv[d] = mn;
+    grids[g].maxv[d] = mx;
+    grids[g].tile[d] = __fdiv_rn(__fsub_rn(mx, mn), (float)grids[g].k);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tile binning: data_structures/detail/AssociationMap.hpp:20-61 with
+// Tiles::GetGlobalBin (Tiles.hpp:208-227, TilesView.hpp:54-64)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, const Chunk* chunks,
+                                                  const EventDesc* events, const GridDesc* grids,
+                                                  int32_t* tile_of, int32_t* point_event,
+                                                  int32_t* tile_count) {
+  __shared__ GridDesc sg;
+  const Chunk c = chunks[blockIdx.x];
+  const EventDesc ev = events[c.event];
+  if (threadIdx.x == 0)
+    sg = grids[ev.grid];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int base = c.begin; base < c.end; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const bool valid = i < c.end;
+    int t = -1;
+    if (valid) {
+      int b = ev.tile_base;
+      for (int d = 0; d < p.D; ++d)
+        b += sg.stride[d] * get_bin(sg, p, x.p[d][i], d);
+      t = b;
+      tile_of[i] = t;
+      point_event[i] = c.event;
+    }
+    const unsigned mask = __match_any_sync(kFull, t);
+    const int leader = __ffs(mask) - 1;
+    if (valid && lane == leader)
+      atomicAdd(&tile_count[t], __popc(mask));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Single-pass exclusive scan with decoupled look-back.
+// Each block takes a ticket (so every predecessor is already running), scans
+// kScanTile elements, publishes its aggregate, then walks back over its
+// predecessors' descriptors until it finds an inclusive prefix.
+// ---------------------------------------------------------------------------
+
+constexpr unsigned long long kFlagAggregate = 1ull << 62;
+constexpr unsigned long long kFlagInclusive = 2ull << 62;
+constexpr unsigned long long kValueMask = 0xffffffffull;
+
+__device__ __forceinline__ void publish(unsigned long long* d, unsigned long long v) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*d);
+  r.store(v, cuda::memory_order_release);
+}
+__device__ __forceinline__ unsigned long long peek(unsigned long long* d) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*d);
+  return r.load(cuda::memory_order_acquire);
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan(const int32_t* in, int32_t* out, int64_t n,
+                                                   unsigned long long* desc, int32_t* ticket,
+                                                   int32_t* total, uint32_t* status) {
+  __shared__ int s_data[kScanTile + kScanTile / 32];
+  __shared__ int s_warp[kThreads / 32];
+  __shared__ int s_bid;
+  __shared__ int s_prefix;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0)
+    s_bid = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int bid = s_bid;
+  const int64_t base = (int64_t)bid * kScanTile;
+  auto pad = [](int k) { return k + (k >> 5); };
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    const int k = j * kThreads + tid;
+    const int64_t g = base + k;
+    s_data[pad(k)] = (g < n) ? in[g] : 0;
+  }
+  __syncthreads();
+  int v[kScanItems];
+  int sum = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    v[j] = s_data[pad(tid * kScanItems + j)];
+    sum += v[j];
+  }
+  // inclusive scan of thread sums
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o)
+      incl += y;
+  }
+  if (lane == 31)
+    s_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = (lane < kThreads / 32) ? s_warp[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, wi, o);
+      if (lane >= o)
+        wi += y;
+    }
+    if (lane < kThreads / 32)
+      s_warp[lane] = wi - w;  // exclusive warp offsets
+    const int aggregate = __shfl_sync(kFull, wi, kThreads / 32 - 1);
+    // publish and look back
+    int exclusive = 0;
+    if (bid == 0) {
+      if (lane == 0)
+        publish(&desc[0], kFlagInclusive | (unsigned)aggregate);
+    } else {
+      if (lane == 0)
+        publish(&desc[bid], kFlagAggregate | (unsigned)aggregate);
+      int pred = bid - 1;
+      bool done = false;
+      while (!done) {
+        const int idx = pred - lane;
+        unsigned long long dsc = kFlagInclusive;  // lanes beyond block 0 contribute nothing
+        if (idx >= 0) {
+          int spins = 0;
+          dsc = peek(&desc[idx]);
+          while ((dsc >> 62) == 0) {
+            if (++spins > kSpinLimit) {
+              atomicOr(status, kStatusScanTimeout);
+              dsc = kFlagInclusive;
+              break;
+            }
+            __nanosleep(64);
+            dsc = peek(&desc[idx]);
+          }
+        }
+        const bool inclusive = (dsc >> 62) == 2 || idx < 0;
+        const unsigned ballot = __ballot_sync(kFull, inclusive);
+        const int first = ballot ? (__ffs(ballot) - 1) : 32;  // nearest inclusive predecessor
+        int val = (lane <= first && idx >= 0) ? (int)(dsc & kValueMask) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          val += __shfl_xor_sync(kFull, val, o);
+        exclusive += val;
+        if (ballot)
+          done = true;
+        else
+          pred -= 32;
+      }
+      if (lane == 0)
+        publish(&desc[bid], kFlagInclusive | (unsigned)(exclusive + aggregate));
+    }
+    if (lane == 0) {
+      s_prefix = exclusive;
+      if (base + kScanTile >= n)
+        *total = exclusive + aggregate;
+    }
+  }
+  __syncthreads();
+  int run = s_prefix + s_warp[warp] + incl - sum;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    s_data[pad(tid * kScanItems + j)] = run;
+    run += v[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    const int k = j * kThreads + tid;
+    const int64_t g = base + k;
+    if (g < n)
+      out[g] = s_data[pad(k)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Scatter and per-tile ordering
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) k_scatter(const int32_t* tile_of, int64_t n,
+                                                      int32_t* cursor, int32_t* perm) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    const bool valid = i < n;
+    const int t = valid ? tile_of[i] : -1;
+    const unsigned mask = __match_any_sync(kFull, t);
+    const int leader = __ffs(mask) - 1;
+    int pos = 0;
+    if (valid && lane == leader)
+      pos = atomicAdd(&cursor[t], __popc(mask));
+    pos = __shfl_sync(kFull, pos, leader);
+    if (valid)
+      perm[pos + __popc(mask & lanemask_lt())] = (int32_t)i;
+  }
+}
+
+// Bitonic sort of s[0..P) (P a power of two) by the whole block.
+__device__ void block_bitonic(int* s, int P) {
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int a = s[i], b = s[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            s[i] = b;
+            s[ixj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Sorts a segment of at most kSortCap ids in place (ascending).
+__device__ void sort_segment(int32_t* seg, int m, int* s) {
+  // Already ascending? (common when one warp scattered the whole tile)
+  int unsorted = 0;
+  for (int i = threadIdx.x; i + 1 < m; i += blockDim.x)
+    unsorted |= seg[i] > seg[i + 1];
+  if (!__syncthreads_or(unsorted))
+    return;
+  int P = 1;
+  while (P < m)
+    P <<= 1;
+  for (int i = threadIdx.x; i < P; i += blockDim.x)
+    s[i] = (i < m) ? seg[i] : INT_MAX;
+  __syncthreads();
+  block_bitonic(s, P);
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    seg[i] = s[i];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offset, int64_t n_tiles,
+                                                        int32_t* perm, int32_t* oversize,
+                                                        int32_t* oversize_count) {
+  __shared__ int s[kSortCap];
+  for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int begin = tile_offset[t], end = tile_offset[t + 1];
+    const int m = end - begin;
+    if (m <= 1)
+      continue;
+    if (m <= kSortCap) {
+      sort_segment(perm + begin, m, s);
+    } else {
+      for (int c = begin; c < end; c += kSortCap)
+        sort_segment(perm + c, min(kSortCap, end - c), s);
+      if (threadIdx.x == 0)
+        oversize[atomicAdd(oversize_count, 1)] = (int32_t)t;
+    }
+  }
+}
+
+// Tiles larger than kSortCap hold sorted chunks of kSortCap ids. Each id's
+// final rank is its rank in its chunk plus, for every other chunk, the number
+// of ids below it (binary search); ids are distinct, so ranks are a permutation.
+__global__ void __launch_bounds__(kThreads) k_tile_merge(const int32_t* tile_offset,
+                                                         const int32_t* oversize,
+                                                         const int32_t* oversize_count,
+                                                         const int32_t* perm, int32_t* tmp) {
+  const int count = *oversize_count;
+  for (int e = blockIdx.x; e < count; e += gridDim.x) {
+    const int t = oversize[e];
+    const int begin = tile_offset[t], end = tile_offset[t + 1];
+    const int m = end - begin;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      const int v = perm[begin + i];
+      const int my_chunk = i / kSortCap;
+      int rank = i - my_chunk * kSortCap;
+      for (int c = 0; c * kSortCap < m; ++c) {
+        if (c == my_chunk)
+          continue;
+        int lo = c * kSortCap, hi = min(m, lo + kSortCap);
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (perm[begin + mid] < v)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        rank += lo - c * kSortCap;
+      }
+      tmp[begin + rank] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_tile_merge_copy(const int32_t* tile_offset,
+                                                              const int32_t* oversize,
+                                                              const int32_t* oversize_count,
+                                                              const int32_t* tmp, int32_t* perm) {
+  const int count = *oversize_count;
+  for (int e = blockIdx.x; e < count; e += gridDim.x) {
+    const int t = oversize[e];
+    for (int i = tile_offset[t] + threadIdx.x; i < tile_offset[t + 1]; i += blockDim.x)
+      perm[i] = tmp[i];
+  }
+}
+
+// Tile-contiguous copy of everything the sweeps read.
+__global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int32_t* perm,
+                                                     CoordPtrs x, const float* w, CoordPtrs sig,
+                                                     int32_t has_sigma, const float* unc,
+                                                     const uint32_t* tags,
+                                                     const int32_t* point_event, float* sx,
+                                                     float* sw, float* ssig, float* sunc,
+                                                     uint32_t* stag, int32_t* sevt) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const int i = perm[s];
+    for (int d = 0; d < D; ++d)
+      sx[d * n + s] = x.p[d][i];
+    sw[s] = w[i];
+    sevt[s] = point_event[i];
+    if (has_sigma)
+      for (int d = 0; d < D; ++d)
+        ssig[d * n + s] = ((has_sigma >> d) & 1) ? sig.p[d][i] : 0.0f;
+    if (unc)
+      sunc[s] = unc[i];
+    if (tags)
+      stag[s] = tags[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Seeds and labels: core/detail/ClusteringKernels.hpp:293-343, :419-446
+// ---------------------------------------------------------------------------
+
+__global__ void k_parent_init(int64_t n, const int32_t* nh, int32_t* parent) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    parent[i] = nh[i] < 0 ? (int32_t)i : nh[i];
+}
+
+// Root of each point's nearest-higher chain by pointer jumping with path
+// halving: every write stores an ancestor, so concurrent updates stay valid
+// and every step moves strictly up the tree.
+__global__ void k_labels(int64_t n, int32_t* parent, const int32_t* seed_flag,
+                         const int32_t* seed_rank, const int32_t* point_event,
+                         int32_t* cluster_index, int32_t* seeds, int32_t* seed_event,
+                         uint32_t* status) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int x = (int)i;
+    int64_t steps = 0;
+    for (;;) {
+      const int px = __ldcg(&parent[x]);
+      if (px == x)
+        break;
+      const int ppx = __ldcg(&parent[px]);
+      if (ppx != px)
+        parent[x] = ppx;
+      x = ppx;
+      if (++steps > n) {
+        atomicOr(status, kStatusLabelTimeout);
+        break;
+      }
+    }
+    cluster_index[i] = seed_flag[x] ? seed_rank[x] : -1;
+    if (seed_flag[i]) {
+      seeds[seed_rank[i]] = (int32_t)i;
+      seed_event[seed_rank[i]] = point_event[i];
+    }
+  }
+}
+
+int grid_for(int64_t n, int per_block = kThreads) {
+  const int64_t b = (n + per_block - 1) / per_block;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+}
+
+cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
+                 const DeviceBuffers& b, cudaStream_t st) {
+  const int blocks = scan_blocks_for(n);
+  cudaError_t e = cudaMemsetAsync(b.scan_desc, 0, sizeof(unsigned long long) * blocks, st);
+  if (e != cudaSuccess)
+    return e;
+  e = cudaMemsetAsync(b.counters, 0, sizeof(int32_t), st);  // ticket
+  if (e != cudaSuccess)
+    return e;
+  if (n == 0)
+    return cudaMemsetAsync(total, 0, sizeof(int32_t), st);
+  k_scan<<<blocks, kThreads, 0, st>>>(in, out, n, b.scan_desc, b.counters, total, b.status);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
+
+cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io,
+                       const DeviceBuffers& b, cudaStream_t st) {
+  const int D = sh.D;
+  const int64_t n = sh.n;
+  CoordPtrs x{}, sig{};
+  for (int d = 0; d < D; ++d) {
+    x.p[d] = io.coords[d];
+    sig.p[d] = io.sigma[d];
+  }
+#define CLUE_CHECK(expr)          \
+  do {                            \
+    cudaError_t e_ = (expr);      \
+    if (e_ != cudaSuccess)        \
+      return e_;                  \
+  } while (0)
+#define CLUE_LAUNCHED() CLUE_CHECK(cudaGetLastError())
+
+  // grid extents
+  k_grid_init<<<(sh.n_grids * kMaxDim + 127) / 128, 128, 0, st>>>(b.grid_minmax, sh.n_grids);
+  CLUE_LAUNCHED();
+  k_minmax<<<sh.n_chunks, kThreads, 0, st>>>(D, x, b.chunks, b.events, b.grid_minmax);
+  CLUE_LAUNCHED();
+  k_grid_finalize<<<(sh.n_grids + 127) / 128, 128, 0, st>>>(D, b.grids, sh.n_grids, b.grid_minmax);
+  CLUE_LAUNCHED();
+
+  // counting sort by tile
+  CLUE_CHECK(cudaMemsetAsync(b.tile_count, 0, sizeof(int32_t) * sh.n_tiles, st));
+  k_bin<<<sh.n_chunks, kThreads, 0, st>>>(prm, x, b.chunks, b.events, b.grids, b.tile_of,
+                                           b.point_event, b.tile_count);
+  CLUE_LAUNCHED();
+  CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));
+  CLUE_CHECK(cudaMemcpyAsync(b.tile_cursor, b.tile_offset, sizeof(int32_t) * sh.n_tiles,
+                             cudaMemcpyDeviceToDevice, st));
+  k_scatter<<<grid_for(n), kThreads, 0, st>>>(b.tile_of, n, b.tile_cursor, b.perm);
+  CLUE_LAUNCHED();
+  CLUE_CHECK(cudaMemsetAsync(b.counters + 2, 0, sizeof(int32_t), st));
+  k_tile_sort<<<(int)std::min<int64_t>(sh.n_tiles, 148 * 32), kThreads, 0, st>>>(
+      b.tile_offset, sh.n_tiles, b.perm, b.oversize, b.counters + 2);
+  CLUE_LAUNCHED();
+  k_tile_merge<<<148, kThreads, 0, st>>>(b.tile_offset, b.oversize, b.counters + 2, b.perm,
+                                         b.merge_tmp);
+  CLUE_LAUNCHED();
+  k_tile_merge_copy<<<148, kThreads, 0, st>>>(b.tile_offset, b.oversize, b.counters + 2,
+                                              b.merge_tmp, b.perm);
+  CLUE_LAUNCHED();
+  k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
+                                             io.unc, io.tags, b.point_event, b.sorted_coords,
+                                             b.sorted_weight, b.sorted_sigma, b.sorted_unc,
+                                             b.sorted_tag, b.sorted_event);
+  CLUE_LAUNCHED();
+
+  // the two sweeps
+  SweepArgs a{};
+  a.n = n;
+  a.events = b.events;
+  a.grids = b.grids;
+  a.tile_offset = b.tile_offset;
+  a.sx = b.sorted_coords;
+  a.sw = b.sorted_weight;
+  a.ssig = b.sorted_sigma;
+  a.sunc = b.sorted_unc;
+  a.stag = b.sorted_tag;
+  a.perm = b.perm;
+  a.sevt = b.sorted_event;
+  a.srho = b.sorted_rho;
+  a.out_rho = io.rho;
+  a.out_nh = io.nh ? io.nh : b.nh;
+  a.out_seed = io.is_seed;
+  a.seed_flag = b.seed_flag;
+  CLUE_CHECK(launch_density(D, prm, a, st));
+  CLUE_CHECK(launch_nearest_higher(D, prm, a, st));
+
+  // seeds and labels
+  CLUE_CHECK(scan(b.seed_flag, b.seed_rank, n, b.counters + 1, b, st));
+  k_parent_init<<<grid_for(n), kThreads, 0, st>>>(n, a.out_nh, b.parent);
+  CLUE_LAUNCHED();
+  k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.seed_flag, b.seed_rank, b.point_event,
+                                             io.cluster_index, b.seeds, b.seed_event, b.status);
+  CLUE_LAUNCHED();
+#undef CLUE_LAUNCHED
+#undef CLUE_CHECK
+  return cudaSuccess;
+}
+
+}  // namespace clue_impl

@@ -1,0 +1,258 @@
+/*
+ * clue_sm100.h — C ABI of libclue_sm100.so, a B200 (sm_100a) implementation of
+ * CLUEstering's `clue::Clusterer<Ndim>::make_clusters` (single event and
+ * batched) and of the result accessors around it.
+ *
+ * The reference has no C ABI: its boundary is the header-only C++20 template
+ * API in include/CLUEstering/core/Clusterer.hpp. Each entry point below names
+ * the reference member it replaces. The C++20 header clue_sm100.hpp rebuilds
+ * that template API (clue::Clusterer, clue::PointsHost, clue::PointsDevice,
+ * the convolutional kernels and the distance metrics) on top of these calls.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only. Streams are passed as `void*` holding a
+ *     cudaStream_t (NULL = the legacy default stream).
+ *   - Every call returns a clue_status. CLUE_ERR_INVALID_ARGUMENT,
+ *     CLUE_ERR_OUT_OF_RANGE and CLUE_ERR_RUNTIME correspond to the reference's
+ *     std::invalid_argument, std::out_of_range and std::runtime_error.
+ *     clue_last_error() returns a message for the calling thread's last error.
+ *   - "_device" entry points take device pointers and are asynchronous on the
+ *     given stream. "_host" entry points take host pointers, copy through
+ *     pinned staging and return with the results in host memory, as the
+ *     reference's PointsHost overloads do.
+ *   - Coordinates, weights and every FP quantity are float32. The index type
+ *     is int32 (the reference's is uint32 for sizes and int32 for ids).
+ *   - A workspace is not thread-safe (like the reference's Clusterer, whose
+ *     tiles and seed buffers are reused between calls). Use one per thread or
+ *     per stream. Different workspaces may run concurrently.
+ */
+#ifndef CLUE_SM100_H
+#define CLUE_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+/* Exported with default visibility even when the library is built with
+ * -fvisibility=hidden. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLUE_MAX_DIM 10
+#define CLUE_ABI_VERSION 1
+
+typedef enum {
+  CLUE_OK = 0,
+  CLUE_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  CLUE_ERR_OUT_OF_RANGE = 2,     /* std::out_of_range */
+  CLUE_ERR_RUNTIME = 3,          /* std::runtime_error */
+  CLUE_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+  CLUE_ERR_OUT_OF_MEMORY = 5,    /* device allocation or admission budget */
+  CLUE_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up */
+  CLUE_ERR_NOT_READY = 7         /* serving: the event has not completed yet */
+} clue_status;
+
+/* Convolutional kernels: core/ConvolutionalKernel.hpp:18-109. */
+typedef enum {
+  CLUE_KERNEL_FLAT = 0,        /* params[0] = flat value (reference default 0.5) */
+  CLUE_KERNEL_EXPONENTIAL = 1, /* params = {exp_avg, exp_amplitude} */
+  CLUE_KERNEL_GAUSSIAN = 2     /* params = {gaus_std, gaus_amplitude} */
+} clue_kernel_kind;
+
+/* Distance metrics: core/DistanceMetrics.hpp:63-318. */
+typedef enum {
+  CLUE_METRIC_EUCLIDEAN = 0,
+  CLUE_METRIC_WEIGHTED_EUCLIDEAN = 1, /* metric_params = per-dimension weights */
+  CLUE_METRIC_PERIODIC_EUCLIDEAN = 2, /* metric_params = per-dimension periods (0 = not periodic) */
+  CLUE_METRIC_MANHATTAN = 3,
+  CLUE_METRIC_CHEBYSHEV = 4,
+  CLUE_METRIC_WEIGHTED_CHEBYSHEV = 5, /* metric_params = per-dimension weights */
+  CLUE_METRIC_MAHALANOBIS = 6         /* needs sigma for every dimension */
+} clue_metric_kind;
+
+/* Tile grid of the batched call. */
+typedef enum {
+  /* One grid from all points of the batch, replicated per event: the
+   * reference's batched semantics (core/Clusterer.hpp:62-68). */
+  CLUE_GRID_SHARED = 0,
+  /* One grid per event from that event's points: every event gets exactly the
+   * result the single-event call would give it, independent of the batch. */
+  CLUE_GRID_PER_EVENT = 1
+} clue_grid_mode;
+
+/* Clustering parameters: the Clusterer constructor arguments
+ * (core/Clusterer.hpp:102-105; dm and seed_dc default to dc there — pass dc),
+ * setWrappedCoordinates (:259-267) and the kernel/metric objects. */
+typedef struct {
+  float dc;      /* density_radius */
+  float rhoc;    /* min_density */
+  float dm;      /* outlier_distance */
+  float seed_dc; /* seeding_distance */
+  uint8_t wrapped[CLUE_MAX_DIM];
+  int32_t kernel_kind;
+  float kernel_params[2];
+  int32_t metric_kind;
+  float metric_params[CLUE_MAX_DIM];
+  int32_t points_per_tile; /* 0 = the reference's 128 (core/Clusterer.hpp:57) */
+} clue_params;
+
+/* One SoA point set (data_structures/internal/PointsCommon.hpp:96-110).
+ * Inputs: coords[d] for d < ndim, weight; optional sigma[d], density_uncertainty
+ * and tags (NULL when unset: PointsHost::set_sigma/set_density_uncertainty/
+ * set_tags). Outputs: cluster_index is required; is_seed, rho and
+ * nearest_higher are optional (NULL = not returned). */
+typedef struct {
+  int32_t ndim;
+  int32_t n;
+  const float* coords[CLUE_MAX_DIM];
+  const float* weight;
+  const float* sigma[CLUE_MAX_DIM];
+  const float* density_uncertainty;
+  const uint32_t* tags;
+  int32_t* cluster_index;
+  int32_t* is_seed;
+  float* rho;
+  int32_t* nearest_higher;
+} clue_points;
+
+typedef struct clue_workspace clue_workspace;
+
+/* ---- library -------------------------------------------------------------- */
+int32_t clue_abi_version(void);
+const char* clue_status_string(clue_status status);
+/* Message of the calling thread's last failed call ("" if none). */
+const char* clue_last_error(void);
+
+/* Parameter validation of the Clusterer constructor and setParameters
+ * (core/detail/Clusterer.hpp:42-48, :81-87) and of the kernel constructors
+ * (core/detail/ConvolutionalKernel.hpp:13-50). */
+clue_status clue_validate_params(const clue_params* params);
+
+/* ---- workspace ------------------------------------------------------------ */
+/* The reusable device state a Clusterer owns (core/Clusterer.hpp:49-51: tiles,
+ * seeds, event associations). Buffers grow on demand and are never shrunk. */
+clue_status clue_workspace_create(clue_workspace** ws, int32_t device);
+clue_status clue_workspace_destroy(clue_workspace* ws);
+/* Bytes of device memory the workspace holds. */
+clue_status clue_workspace_bytes(const clue_workspace* ws, size_t* bytes);
+/* Device bytes a run over n points / n_tiles tiles would need (admission). */
+size_t clue_workspace_bytes_for(int32_t ndim, int64_t n_points, int64_t n_tiles, int32_t n_events);
+
+/* ---- clustering ----------------------------------------------------------- */
+/* Clusterer::make_clusters(Queue&, PointsDevice&, metric, kernel)
+ * (core/detail/Clusterer.hpp:139-151). Device pointers; asynchronous. */
+clue_status clue_make_clusters_device(clue_workspace* ws, const clue_params* params,
+                                      const clue_points* points, void* stream);
+
+/* Clusterer::make_clusters(Queue&, PointsHost&, [PointsDevice&,] metric, kernel)
+ * (core/detail/Clusterer.hpp:90-138). Host pointers; returns synchronised. */
+clue_status clue_make_clusters_host(clue_workspace* ws, const clue_params* params,
+                                    const clue_points* points, void* stream);
+
+/* Clusterer::make_clusters(Queue&, PointsDevice&, span<const uint32_t> batch_item_sizes,
+ * metric, kernel) (core/detail/Clusterer.hpp:170-183). event_sizes is a host
+ * array of n_events sizes summing to points->n. Device pointers; asynchronous. */
+clue_status clue_make_clusters_batched_device(clue_workspace* ws, const clue_params* params,
+                                              const clue_points* points,
+                                              const uint32_t* event_sizes, int32_t n_events,
+                                              int32_t grid_mode, void* stream);
+
+/* Clusterer::make_clusters(Queue&, PointsHost&, PointsDevice&, span<const uint32_t>,
+ * metric, kernel) (core/detail/Clusterer.hpp:153-168). Host pointers. */
+clue_status clue_make_clusters_batched_host(clue_workspace* ws, const clue_params* params,
+                                            const clue_points* points,
+                                            const uint32_t* event_sizes, int32_t n_events,
+                                            int32_t grid_mode, void* stream);
+
+/* ---- results of the last run ---------------------------------------------- */
+/* Number of clusters (= seeds) of the last run; waits for it to finish.
+ * PointsHost::n_clusters / PointsDevice::n_clusters
+ * (data_structures/detail/PointsHost.hpp:106-116, detail/PointsDevice.hpp:109-123). */
+clue_status clue_n_clusters(clue_workspace* ws, int32_t* n_clusters);
+
+/* Clusterer::getSeeds (core/detail/Clusterer.hpp:197-203): seed indices of the
+ * last run in ascending order (cluster id k is seeds[k]). Copies up to
+ * capacity entries to host memory; CLUE_ERR_RUNTIME before the first run. */
+clue_status clue_get_seeds(clue_workspace* ws, int32_t* seeds, int32_t capacity,
+                           int32_t* n_seeds);
+
+/* Clusterer::getClusters / clue::get_clusters (utils/detail/get_clusters.hpp:24-49):
+ * cluster -> points map of the last run as CSR on the device. offsets has
+ * n_clusters + 1 entries, points has room for every clustered point; point
+ * ids within a cluster are ascending. Asynchronous on stream. */
+clue_status clue_get_clusters_device(clue_workspace* ws, int32_t* offsets, int32_t* points,
+                                     void* stream);
+
+/* Clusterer::getSampleAssociations (core/detail/Clusterer.hpp:219-242): event
+ * -> cluster ids of the last batched run, as CSR in host memory. offsets has
+ * n_events + 1 entries; cluster ids of event e are offsets[e]..offsets[e+1]-1
+ * (ids are grouped by event). n_keys receives the number of keys the reference's
+ * associator reports (1 + the last event that has a cluster). */
+clue_status clue_sample_associations(clue_workspace* ws, int32_t* offsets, int32_t capacity,
+                                     int32_t* n_keys);
+
+/* ---- streams and memory (used by the C++ header; no CUDA headers needed) -- */
+clue_status clue_stream_create(void** stream, int32_t device);
+clue_status clue_stream_destroy(void* stream);
+clue_status clue_stream_synchronize(void* stream);
+clue_status clue_device_malloc(void** ptr, size_t bytes, int32_t device);
+clue_status clue_device_free(void* ptr);
+clue_status clue_host_malloc_pinned(void** ptr, size_t bytes);
+clue_status clue_host_free_pinned(void* ptr);
+/* kind: 0 host->device, 1 device->host, 2 device->device. Asynchronous. */
+clue_status clue_memcpy_async(void* dst, const void* src, size_t bytes, int32_t kind, void* stream);
+
+/* ---- serving -------------------------------------------------------------- */
+/* A request loop with continuous batching: events are submitted from host
+ * memory as they arrive, admitted while their device footprint fits the
+ * memory budget, grouped by size into batches that run concurrently on
+ * several streams, and completed individually. Each event gets the
+ * single-event result (CLUE_GRID_PER_EVENT semantics), so its result does not
+ * depend on what it was batched with. */
+typedef struct clue_server clue_server;
+
+typedef struct {
+  int32_t device;
+  int32_t ndim;          /* all events of a server share ndim and params */
+  size_t budget_bytes;   /* device memory the server may hold for in-flight work */
+  int32_t max_inflight;  /* batches in flight at once (streams) */
+  int32_t max_batch_events;
+  int64_t max_batch_points;
+  int32_t linger_us;     /* how long a partial batch may wait for company */
+} clue_server_config;
+
+typedef struct {
+  int64_t submitted, completed, batches;
+  int64_t points_completed;
+  int64_t inflight_bytes_peak;
+  double latency_p50_ms, latency_p99_ms, latency_max_ms;
+} clue_server_stats;
+
+clue_status clue_server_create(clue_server** server, const clue_server_config* config,
+                               const clue_params* params);
+/* Queues one event; the host buffers must stay valid until it completes.
+ * Outputs land in points->cluster_index (and the optional outputs). */
+clue_status clue_server_submit(clue_server* server, const clue_points* points, uint64_t* ticket);
+/* CLUE_OK when the event completed, CLUE_ERR_NOT_READY otherwise. */
+clue_status clue_server_poll(clue_server* server, uint64_t ticket);
+/* Waits until every submitted event has completed. */
+clue_status clue_server_drain(clue_server* server);
+clue_status clue_server_stats_get(clue_server* server, clue_server_stats* stats);
+/* Per-event latencies (completion - submission, ms) in ticket order. */
+clue_status clue_server_latencies(clue_server* server, double* latencies_ms, int64_t capacity,
+                                  int64_t* count);
+clue_status clue_server_destroy(clue_server* server);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* CLUE_SM100_H */

@@ -1,0 +1,317 @@
+"""GPU parity: libclue_sm100.so (through the C ABI) against the CPU checker.
+
+The bar is bit-exact equality of every output — density (compared as bits),
+nearest higher, seed flags and cluster ids — on the same seeded inputs. The
+checker evaluates the Gaussian/exponential kernels with the library-owned
+exponential (clue_expf) that the GPU path uses.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import cluestering_b200 as clue
+from cluestering_b200 import workloads as W
+from oracle import oracle as O
+from tests.helpers import fixture, same_partition, truth_count
+
+pytestmark = pytest.mark.gpu
+
+METRIC_CLASSES = {
+    "euclidean": lambda p: clue.EuclideanMetric(),
+    "weighted_euclidean": lambda p: clue.WeightedEuclideanMetric(*p),
+    "periodic_euclidean": lambda p: clue.PeriodicEuclideanMetric(*p),
+    "manhattan": lambda p: clue.ManhattanMetric(),
+    "chebyshev": lambda p: clue.ChebyshevMetric(),
+    "weighted_chebyshev": lambda p: clue.WeightedChebyshevMetric(*p),
+    "mahalanobis": lambda p: clue.MahalanobisMetric(),
+}
+KERNEL_CLASSES = {
+    "flat": lambda p: clue.FlatKernel(*p),
+    "gaussian": lambda p: clue.GaussianKernel(*p),
+    "exponential": lambda p: clue.ExponentialKernel(*p),
+}
+
+
+def run_gpu(coords, weights, dc, rhoc, dm=None, seed_dc=None, *, metric="euclidean", metric_params=(),
+            kernel="flat", kernel_params=(0.5,), sigma=None, unc=None, tags=None, wrapped=None,
+            sizes=None, grid_mode=clue.GRID_SHARED, path="host", clusterer=None):
+    c = clusterer or clue.Clusterer(dc, rhoc, dm, seed_dc)
+    if clusterer is not None:
+        c.setParameters(dc, rhoc, dm, seed_dc)
+    if wrapped is not None:
+        c.setWrappedCoordinates(*wrapped)
+    m = METRIC_CLASSES[metric](metric_params)
+    k = KERNEL_CLASSES[kernel](kernel_params)
+    coords = np.ascontiguousarray(coords, np.float32)
+    if coords.ndim == 1:
+        coords = coords[None]
+    D, n = coords.shape
+    if path == "host":
+        pts = clue.PointsHost(coords, weights)
+        pts.is_seed = np.zeros(n, np.int32)
+        pts.rho = np.zeros(n, np.float32)
+        pts.nearest_higher = np.zeros(n, np.int32)
+        if sigma is not None:
+            for d, s in enumerate(sigma):
+                if s is not None:
+                    pts.set_sigma(d, s)
+        if unc is not None:
+            pts.set_density_uncertainty(unc)
+        if tags is not None:
+            pts.set_tags(tags)
+        c.make_clusters(pts, m, k, batch_item_sizes=sizes, grid_mode=grid_mode)
+        out = dict(rho=pts.rho, nh=pts.nearest_higher, seed=pts.is_seed, ci=pts.cluster_index)
+    else:
+        import torch
+        dev = torch.device("cuda:0")
+        t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+        pts = clue.PointsDevice(
+            t(coords), t(weights),
+            sigma=None if sigma is None else [None if s is None else t(s) for s in sigma],
+            density_uncertainty=None if unc is None else t(unc),
+            tags=None if tags is None else t(np.asarray(tags, np.int64).astype(np.int32), torch.int32))
+        c.make_clusters(pts, m, k, batch_item_sizes=sizes, grid_mode=grid_mode)
+        out = dict(rho=pts.rho.cpu().numpy(), nh=pts.nearest_higher.cpu().numpy(),
+                   seed=pts.is_seed.cpu().numpy(), ci=pts.cluster_index.cpu().numpy())
+    out["clusterer"] = c
+    return out
+
+
+def run_oracle(coords, weights, dc, rhoc, dm=None, seed_dc=None, *, metric="euclidean", metric_params=(),
+               kernel="flat", kernel_params=(0.5,), sigma=None, unc=None, tags=None, wrapped=None,
+               sizes=None, grid_mode=clue.GRID_SHARED, threads=8):
+    kw = dict(metric=metric, metric_params=list(metric_params), kernel=kernel,
+              kernel_params=tuple(kernel_params), sigma=sigma, unc=unc, tags=tags, wrapped=wrapped,
+              exp_mode=O.EXP_CLUE, n_threads=threads)
+    if sizes is None:
+        return O.make_clusters(coords, weights, dc, rhoc, dm, seed_dc, **kw)
+    return O.make_clusters_batched(coords, weights, sizes, dc, rhoc, dm, seed_dc,
+                                   shared_grid=(grid_mode == clue.GRID_SHARED), **kw)
+
+
+def assert_identical(g, o):
+    assert np.array_equal(g["rho"].view(np.int32), o.rho.view(np.int32)), \
+        f"rho differs at {np.nonzero(g['rho'].view(np.int32) != o.rho.view(np.int32))[0][:10]}"
+    assert np.array_equal(g["nh"], o.nearest_higher), \
+        f"nearest higher differs at {np.nonzero(g['nh'] != o.nearest_higher)[0][:10]}"
+    assert np.array_equal(g["seed"], o.is_seed)
+    assert np.array_equal(g["ci"], o.cluster_index)
+
+
+def check(coords, weights, *args, **kw):
+    g = run_gpu(coords, weights, *args, **kw)
+    kw.pop("path", None)
+    kw.pop("clusterer", None)
+    o = run_oracle(coords, weights, *args, **kw)
+    assert_identical(g, o)
+    return g, o
+
+
+# ---- the benchmark configurations -------------------------------------------------------------
+
+@pytest.mark.parametrize("path", ["host", "device"])
+def test_single_2d_event(path):
+    ev = W.single_2d()
+    g, o = check(ev.coords, ev.weights, 1.5, 5.0, 1.5, path=path)
+    assert o.n_clusters >= 15
+
+
+def test_layered_3d_event_gaussian_kernel():
+    ev = W.layered_3d()
+    check(ev.coords, ev.weights, 3.0, 10.0, 4.0, kernel="gaussian", kernel_params=(1.0, 1.0))
+
+
+def test_large_2d_event_exponential_weights_reduced():
+    ev = W.blobs(1 << 17, 250, 0.0, 353.0, 1.0, 0.1, seed=9, weights="exponential")
+    check(ev.coords, ev.weights, 1.5, 8.0, 2.0)
+
+
+def test_large_2d_event_full_size():
+    ev = W.large_2d()
+    check(ev.coords, ev.weights, 1.5, 8.0, 2.0, path="device")
+
+
+def test_batch_of_mixed_size_events_per_event_grid():
+    ev, sizes = W.batch_2d(64, 256, 8192, seed=21)
+    w = np.random.default_rng(3).exponential(1.0, ev.n).astype(np.float32)
+    check(ev.coords, w, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT)
+
+
+def test_batch_of_mixed_size_events_shared_grid():
+    ev, sizes = W.batch_2d(16, 256, 4096, seed=22)
+    w = np.random.default_rng(4).exponential(1.0, ev.n).astype(np.float32)
+    check(ev.coords, w, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_SHARED)
+
+
+def test_batch_events_alone_and_in_the_mix():
+    ev, sizes = W.batch_2d(12, 256, 6000, seed=23)
+    w = np.random.default_rng(5).exponential(1.0, ev.n).astype(np.float32)
+    mix = run_gpu(ev.coords, w, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT)
+    begin, label0 = 0, 0
+    for s in sizes.tolist():
+        one = run_gpu(ev.coords[:, begin:begin + s], w[begin:begin + s], 1.5, 5.0, 1.5)
+        sl = slice(begin, begin + s)
+        assert np.array_equal(mix["rho"][sl].view(np.int32), one["rho"].view(np.int32))
+        assert np.array_equal(mix["nh"][sl], np.where(one["nh"] >= 0, one["nh"] + begin, -1))
+        assert np.array_equal(mix["ci"][sl], np.where(one["ci"] >= 0, one["ci"] + label0, -1))
+        begin += s
+        label0 += int(one["ci"].max()) + 1
+
+
+# ---- metrics, kernels and per-point options ---------------------------------------------------
+
+@pytest.mark.parametrize("metric,params", [
+    ("euclidean", ()), ("weighted_euclidean", (0.5, 2.0)), ("periodic_euclidean", (0.0, 100.0)),
+    ("manhattan", ()), ("chebyshev", ()), ("weighted_chebyshev", (0.7, 1.3)), ("mahalanobis", ()),
+])
+def test_every_metric(metric, params):
+    ev = W.blobs(6000, 12, 0.0, 100.0, 1.0, 0.1, seed=31)
+    sigma = None
+    if metric == "mahalanobis":
+        rng = np.random.default_rng(7)
+        sigma = [rng.uniform(0.5, 1.5, ev.n).astype(np.float32) for _ in range(2)]
+    check(ev.coords, ev.weights, 1.5, 5.0, 1.5, metric=metric, metric_params=params, sigma=sigma)
+
+
+@pytest.mark.parametrize("kernel,params", [("flat", (0.5,)), ("flat", (1.0,)), ("gaussian", (0.8, 2.0)),
+                                           ("exponential", (1.2, 0.7))])
+def test_every_kernel_with_real_weights(kernel, params):
+    ev = W.blobs(5000, 10, 0.0, 60.0, 1.0, 0.1, seed=32, weights="exponential")
+    check(ev.coords, ev.weights, 1.5, 3.0, 2.0, kernel=kernel, kernel_params=params)
+
+
+def test_wrapped_coordinates_with_periodic_metric():
+    rng = np.random.default_rng(8)
+    ang = np.concatenate([rng.normal(0.05, 0.05, 400), rng.normal(2 * np.pi - 0.05, 0.05, 400)])
+    ang = np.mod(ang, 2 * np.pi)
+    r = rng.uniform(0, 1, ang.size)
+    coords = np.stack([r, ang]).astype(np.float32)
+    w = np.ones(ang.size, np.float32)
+    check(coords, w, 0.2, 5.0, 0.2, metric="periodic_euclidean", metric_params=(0.0, 2 * np.pi),
+          wrapped=[0, 1])
+
+
+def test_sigma_widens_the_search_box():
+    ev = W.blobs(4000, 8, 0.0, 50.0, 1.0, 0.1, seed=33, weights="exponential")
+    rng = np.random.default_rng(9)
+    sigma = [rng.uniform(0.0, 3.0, ev.n).astype(np.float32), None]
+    check(ev.coords, ev.weights, 1.0, 3.0, 1.5, sigma=sigma)
+
+
+def test_density_uncertainty_and_tags():
+    ev = W.blobs(5000, 10, 0.0, 80.0, 1.0, 0.1, seed=34)
+    rng = np.random.default_rng(10)
+    unc = (1.0 + rng.normal(0, 0.3, ev.n)).astype(np.float32)
+    tags = rng.permutation(ev.n).astype(np.uint32)
+    check(ev.coords, ev.weights, 1.5, 5.0, 1.5, unc=unc, tags=tags)
+
+
+def test_seeding_distance_differs_from_outlier_distance():
+    ev = W.blobs(5000, 10, 0.0, 80.0, 1.0, 0.1, seed=35, weights="exponential")
+    check(ev.coords, ev.weights, 1.0, 4.0, 1.5, 3.0)
+    check(ev.coords, ev.weights, 1.0, 4.0, 3.0, 1.2)
+
+
+@pytest.mark.parametrize("D", [1, 3, 4, 7, 10])
+def test_dimensions(D):
+    ev = W.blobs(3000 if D < 7 else 2000, 6, 0.0, 30.0, 1.0, 0.1, seed=40 + D, ndim=D,
+                 weights="exponential")
+    check(ev.coords, ev.weights, 1.5 if D < 4 else 3.0, 2.0, 2.0)
+
+
+# ---- the reference's known-answer tests through the GPU path ----------------------------------
+
+def test_tag_tie_break():
+    coords = np.zeros((2, 2), np.float32)
+    w = np.ones(2, np.float32)
+    g = run_gpu(coords, w, 1.0, 0.0, 1.0)
+    assert g["nh"].tolist() == [1, -1] and g["seed"].tolist() == [0, 1]
+    g = run_gpu(coords, w, 1.0, 0.0, 1.0, tags=np.array([100, 1], np.uint32))
+    assert g["nh"].tolist() == [-1, 0] and g["seed"].tolist() == [1, 0]
+
+
+def test_mahalanobis_merge():
+    coords = np.array([[2.0, 4.0]], np.float32)
+    w = np.ones(2, np.float32)
+    assert run_gpu(coords, w, 1.0, 0.3)["ci"].max() + 1 == 2
+    g = run_gpu(coords, w, 1.0, 0.3, metric="mahalanobis", sigma=[np.array([2.0, 2.0], np.float32)])
+    assert g["ci"].max() + 1 == 1
+
+
+def test_opposite_angles_single_cluster():
+    c, w = fixture("opposite_angles")
+    two_pi = float(np.float32(2.0) * np.float32(math.pi))
+    g, o = check(c, w, 0.2, 5.0, 0.2, wrapped=[0, 1], metric="periodic_euclidean",
+                 metric_params=(0.0, two_pi))
+    assert g["ci"].max() + 1 == 1
+
+
+def test_batched_fixed_batch_size_counts():
+    c, w = fixture("batched_data_1024")
+    g, o = check(c, w, 1.3, 10.0, 1.3, sizes=[1024] * 10)
+    assert g["ci"].max() + 1 == 10 * truth_count("data_1024")
+    offsets, n_keys = g["clusterer"].getSampleAssociations()
+    assert n_keys == 10
+    assert offsets[-1] == g["ci"].max() + 1
+    seeds = g["clusterer"].getSeeds()
+    assert np.array_equal(seeds, o.seeds)
+
+
+@pytest.mark.parametrize("name", ["data_4096", "data_32768"])
+def test_reference_datasets(name):
+    c, w = fixture(name)
+    check(c, w, 1.5, 10.0, 1.5)
+
+
+# ---- edge cases ---------------------------------------------------------------------------------
+
+def test_single_point():
+    g, o = check(np.array([[3.0], [4.0]], np.float32), np.ones(1, np.float32), 1.0, 0.5)
+    assert g["ci"].tolist() == [0]
+
+
+def test_all_points_identical_oversize_tile():
+    # Zero extent in every dimension: every point falls in tile 0, a tile
+    # larger than one shared-memory sort pass.
+    n = 9000
+    coords = np.full((2, n), 7.0, np.float32)
+    w = np.random.default_rng(11).exponential(1.0, n).astype(np.float32)
+    check(coords, w, 1.0, 2.0)
+
+
+def test_dense_blob_in_one_tile():
+    rng = np.random.default_rng(12)
+    coords = np.concatenate([rng.normal(50, 0.05, (2, 12000)), rng.uniform(0, 100, (2, 2000))],
+                            axis=1).astype(np.float32)
+    w = rng.exponential(1.0, coords.shape[1]).astype(np.float32)
+    check(coords, w, 0.05, 1.0, 0.1)
+
+
+def test_no_seeds_when_rhoc_is_unreachable():
+    ev = W.single_2d(3000, seed=5)
+    g, o = check(ev.coords, ev.weights, 1.5, 1e9, 1.5)
+    assert (g["ci"] == -1).all()
+
+
+def test_zero_rhoc():
+    ev = W.single_2d(3000, seed=6)
+    check(ev.coords, ev.weights, 1.5, 0.0, 1.5)
+
+
+def test_workspace_reuse_across_sizes():
+    c = clue.Clusterer(1.5, 5.0, 1.5)
+    for n, seed in [(20000, 1), (2000, 2), (50000, 3), (100, 4)]:
+        ev = W.single_2d(n, seed=seed)
+        g = run_gpu(ev.coords, ev.weights, 1.5, 5.0, 1.5, clusterer=c)
+        assert_identical(g, run_oracle(ev.coords, ev.weights, 1.5, 5.0, 1.5))
+
+
+def test_host_and_device_entry_points_agree():
+    ev = W.single_2d(8000, seed=7)
+    a = run_gpu(ev.coords, ev.weights, 1.5, 5.0, 1.5, path="host")
+    b = run_gpu(ev.coords, ev.weights, 1.5, 5.0, 1.5, path="device")
+    for k in ("rho", "nh", "seed", "ci"):
+        assert np.array_equal(a[k], b[k])
+    assert same_partition(a["ci"], b["ci"])
