@@ -1,0 +1,384 @@
+"""Benchmark of libclue_sm100.so on one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one batched make_clusters over the batch_2d workload: 4,096 2-D
+events of log-uniform size in [256, 65,536] (~48 M points), unit weights,
+dc = 1.5, rhoc = 5, dm = 1.5, flat kernel, one tile grid per event. Inputs are
+larger than L2 (126 MB), so no flush is needed between steps.
+
+`value` is points/s with the inputs resident in HBM (device entry point);
+`e2e` is the same metric through the host entry point with pinned host buffers,
+so every step includes the host->device copy of coordinates and weights and the
+device->host copy of the cluster ids. Extra keys report the plain per-event GPU
+form (one make_clusters call per event with a host sync per event, the
+reference's usage pattern), the 1,048,576-point single event and the serving
+loop. With --impl reference the CPU restatement of the reference algorithm
+(oracle/) runs the same workload on all host cores.
+
+Under torchrun every rank clusters its own batch (events are independent: no
+collective on the data path); time is the max over ranks and `value` the points
+of all ranks divided by it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "points/s batched+served vs plain per-event on same GPU; p50/p99 event latency"
+CONFIG = {
+    "workload": "batch_2d: 4096 2-D events, sizes log-uniform [256, 65536], 20*n/16384 blobs "
+                "(sigma 1) in [0,100]^2 + 10% noise, unit weights; dc=1.5 rhoc=5 dm=1.5 flat(0.5), "
+                "Euclidean; one tile grid per event",
+    "l2": "inputs (~0.58 GB) exceed L2; no flush",
+}
+# Kernel launches of one run (grid init, extents, grid finalize, bin, scan,
+# scatter, tile sort, tile merge, merge copy, gather, density, nearest higher,
+# seed scan, parent init, labels).
+LAUNCHES_PER_RUN = 15
+# Algorithmic bytes per point (4-byte values), 2-D: density reads coordinates
+# and weight and writes rho (4D + 8); nearest higher reads coordinates, rho and
+# index and writes nh (4D + 12); the whole pipeline moves 20D + 64.
+BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4 * D + 12,
+                   "pipeline": lambda D: 20 * D + 64}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference(ev, sizes, budget_points: int, threads: int):
+    """Times the CPU restatement on the first events of the batch (bounded sample)."""
+    from oracle import oracle as O
+    total, k = 0, 0
+    while k < len(sizes) and total + int(sizes[k]) <= budget_points:
+        total += int(sizes[k])
+        k += 1
+    k = max(k, 1)
+    total = int(sizes[:k].sum())
+    t0 = time.perf_counter()
+    O.make_clusters_batched(ev.coords[:, :total], ev.weights[:total], sizes[:k], 1.5, 5.0, 1.5,
+                            shared_grid=False, n_threads=threads)
+    dt = time.perf_counter() - t0
+    return total / dt, f"first {k} events of the batch ({total} points), all events clustered", total
+
+
+def run_reference(args, world, rank):
+    from cluestering_b200 import workloads as W
+    if rank != 0:
+        return 0
+    ev, sizes = W.batch_2d()
+    threads = os.cpu_count() or 1
+    budget = args.cpu_sample_points
+    for _ in range(args.warmup):
+        cpu_reference(ev, sizes, budget // 4, threads)
+    vals = []
+    for _ in range(args.steps):
+        v, sample, pts = cpu_reference(ev, sizes, budget, threads)
+        vals.append(v)
+    value = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": pts / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import cluestering_b200 as clue
+    from cluestering_b200 import _lib as L
+    from cluestering_b200 import workloads as W
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    hbm_peak, peak_kind = measured_peaks()
+
+    # ---- workload, resident in HBM --------------------------------------------------------------
+    ev, sizes = W.batch_2d(seed=3 + 1000 * rank)
+    n_total = int(sizes.sum())
+    coords_d = torch.from_numpy(ev.coords).to(dev)
+    weights_d = torch.from_numpy(ev.weights).to(dev)
+    pts = clue.PointsDevice(coords_d, weights_d, outputs=("cluster_index",))
+    algo = clue.Clusterer(1.5, 5.0, 1.5, device=local)
+
+    def step():
+        algo.make_clusters(pts, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=stream,
+                           synchronize=False)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    barrier(world)
+    ms_max = max_over_ranks(ms, world)
+    value = n_total * world / (ms_max * 1e-3)
+    n_clusters = algo.n_clusters()
+
+    # ---- stage times of one profiled run (outside the timed region) -----------------------------
+    algo.set_profiling(True)
+    step()
+    stage = algo.stage_ms()
+    algo.set_profiling(False)
+    dom = max(("density", "nearest_higher"), key=lambda k: stage[k])
+    D = 2
+    achieved = BYTES_PER_POINT[dom](D) * n_total / (stage[dom] * 1e-3) / 1e9
+
+    # ---- end to end through the host entry point ------------------------------------------------
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    h = clue.PointsHost(pin(ev.coords), pin(ev.weights))
+    h.cluster_index = pin(np.zeros(n_total, np.int32))
+    algo_h = clue.Clusterer(1.5, 5.0, 1.5, device=local)
+    hstream = torch.cuda.Stream(device=dev)
+    for _ in range(max(1, args.warmup // 2)):
+        algo_h.make_clusters(h, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=hstream)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        algo_h.make_clusters(h, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=hstream)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_value = n_total * world / (e2e_ms * 1e-3)
+    same = bool(np.array_equal(h.cluster_index, pts.cluster_index.cpu().numpy()))
+
+    extras = {}
+    if rank == 0 and not args.skip_extras:
+        extras = run_extras(args, ev, sizes, local, stream, hbm_peak)
+
+    if rank != 0:
+        return 0
+    cpu_val, cpu_sample, _ = cpu_reference(ev, sizes, args.cpu_sample_points, os.cpu_count() or 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(CONFIG, points_per_step=n_total * world, events_per_step=len(sizes) * world,
+                       parallelism=f"replicas x{world} (events sharded by rank, no collective)"),
+        "e2e": {"value": e2e_value, "unit": "points/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(ev.coords.nbytes + ev.weights.nbytes),
+                "d2h_bytes_per_step": int(n_total * 4), "matches_device_path": same},
+        "gpu_launches": LAUNCHES_PER_RUN * args.steps,
+        "n_clusters": n_clusters,
+        "stage_ms": {k: round(v, 4) for k, v in stage.items()},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                     "peak_kind": peak_kind,
+                     "note": "sweeps are FP32-issue bound: each point tests ~10^3 candidates in "
+                             "the reference's tile order; bytes are the algorithmic minimum"},
+        "clocks": clocks.summary(),
+        "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": os.cpu_count() or 1,
+                         "kind": "port", "sample": cpu_sample},
+    }
+    line.update(extras)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_extras(args, ev, sizes, local, stream, hbm_peak):
+    """Plain per-event GPU form, the 1M-point single event and (when present) serving."""
+    import torch
+
+    import cluestering_b200 as clue
+    from cluestering_b200 import workloads as W
+
+    out = {}
+    dev = torch.device("cuda", local)
+    # plain per-event: one device call per event and a host sync after each
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    n_ev = min(len(sizes), args.plain_events)
+    views = []
+    coords_d = torch.from_numpy(ev.coords).to(dev)
+    weights_d = torch.from_numpy(ev.weights).to(dev)
+    for e in range(n_ev):
+        a, b = int(offs[e]), int(offs[e + 1])
+        views.append(clue.PointsDevice(coords_d[:, a:b], weights_d[a:b], outputs=("cluster_index",)))
+    algo = clue.Clusterer(1.5, 5.0, 1.5, device=local)
+    for v in views[:8]:
+        algo.make_clusters(v, stream=stream)
+    lat = []
+    t0 = time.perf_counter()
+    for v in views:
+        t1 = time.perf_counter()
+        algo.make_clusters(v, stream=stream)  # synchronises
+        lat.append((time.perf_counter() - t1) * 1e3)
+    dt = time.perf_counter() - t0
+    pts_plain = int(offs[n_ev])
+    out["plain_per_event"] = {"value": pts_plain / dt, "unit": "points/s", "events": n_ev,
+                              "latency_p50_ms": float(np.percentile(lat, 50)),
+                              "latency_p99_ms": float(np.percentile(lat, 99))}
+    del views, coords_d, weights_d
+
+    # single large event (1,048,576 points, exponential weights)
+    big = W.large_2d()
+    bc = torch.from_numpy(big.coords).to(dev)
+    bw = torch.from_numpy(big.weights).to(dev)
+    bp = clue.PointsDevice(bc, bw, outputs=("cluster_index",))
+    algo1 = clue.Clusterer(1.5, 8.0, 2.0, device=local)
+    for _ in range(3):
+        algo1.make_clusters(bp, stream=stream)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    reps = 10
+    for _ in range(reps):
+        algo1.make_clusters(bp, stream=stream, synchronize=False)
+    e.record(stream)
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    algo1.set_profiling(True)
+    algo1.make_clusters(bp, stream=stream)
+    st = algo1.stage_ms()
+    nb = BYTES_PER_POINT["pipeline"](2) * big.n
+    out["single_event_1M"] = {
+        "ms": ms, "points_per_s": big.n / (ms * 1e-3),
+        "hbm_frac_pipeline": nb / (ms * 1e-3) / 1e9 / hbm_peak,
+        "stage_ms": {k: round(v, 4) for k, v in st.items()},
+        "density_gbs": BYTES_PER_POINT["density"](2) * big.n / (st["density"] * 1e-3) / 1e9,
+        "nearest_higher_gbs": BYTES_PER_POINT["nearest_higher"](2) * big.n / (st["nearest_higher"] * 1e-3) / 1e9,
+    }
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-points", type=int, default=3_000_000)
+    ap.add_argument("--plain-events", type=int, default=4096)
+    ap.add_argument("--skip-extras", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # CPU arm: rank 0 times the CPU restatement; other ranks have no work.
+        return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")),
+                             int(os.environ.get("RANK", "0")))
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

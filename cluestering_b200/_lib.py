@@ -24,6 +24,7 @@ KERNEL_FLAT, KERNEL_EXPONENTIAL, KERNEL_GAUSSIAN = 0, 1, 2
 (METRIC_EUCLIDEAN, METRIC_WEIGHTED_EUCLIDEAN, METRIC_PERIODIC_EUCLIDEAN, METRIC_MANHATTAN,
  METRIC_CHEBYSHEV, METRIC_WEIGHTED_CHEBYSHEV, METRIC_MAHALANOBIS) = range(7)
 GRID_SHARED, GRID_PER_EVENT = 0, 1
+STAGES = ("extents", "tiles", "gather", "density", "nearest_higher", "labels")
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libclue_sm100.so")
 
@@ -95,6 +96,8 @@ SIGNATURES = {
     "clue_workspace_destroy": (C.c_int, [_P]),
     "clue_workspace_bytes": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
     "clue_workspace_bytes_for": (C.c_size_t, [C.c_int32, C.c_int64, C.c_int64, C.c_int32]),
+    "clue_workspace_set_profiling": (C.c_int, [_P, C.c_int32]),
+    "clue_workspace_stage_ms": (C.c_int, [_P, _P, C.c_int32]),
     "clue_make_clusters_device": (C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P]),
     "clue_make_clusters_host": (C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P]),
     "clue_make_clusters_batched_device": (

@@ -396,6 +396,15 @@ class Clusterer:
         L.check(L.load().clue_sample_associations(self._ws, offs.ctypes.data, B + 1, C.byref(nk)))
         return offs, nk.value
 
+    def set_profiling(self, enable: bool = True) -> None:
+        L.check(L.load().clue_workspace_set_profiling(self._workspace(), int(enable)))
+
+    def stage_ms(self) -> dict:
+        """Device time of each stage of the last run (needs set_profiling)."""
+        ms = (C.c_float * len(L.STAGES))()
+        L.check(L.load().clue_workspace_stage_ms(self._ws, ms, len(L.STAGES)))
+        return dict(zip(L.STAGES, list(ms)))
+
     def workspace_bytes(self) -> int:
         b = C.c_size_t()
         L.check(L.load().clue_workspace_bytes(self._workspace(), C.byref(b)))

@@ -443,7 +443,7 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   io.rho = pts->rho;
   io.nh = pts->nearest_higher;
   const RunParams prm = make_run_params(params, pts);
-  if ((e = launch_run(sh, prm, io, ws->b, st)) != cudaSuccess)
+  if ((e = launch_run(sh, prm, io, ws->b, st, ws->profiling ? ws->marks : nullptr)) != cudaSuccess)
     return fail_cuda(e, "kernel launch");
   // Seed count and status word come back with the run (read when needed).
   cudaMemcpyAsync(&ws->info->n_seeds, ws->b.counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -630,7 +630,41 @@ clue_status clue_workspace_destroy(clue_workspace* ws) {
     cudaEventDestroy(ws->run_event);
   if (ws->staging_event)
     cudaEventDestroy(ws->staging_event);
+  for (auto& m : ws->marks)
+    if (m)
+      cudaEventDestroy(m);
   delete ws;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_set_profiling(clue_workspace* ws, int32_t enable) {
+  if (!ws)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");
+  if (enable && !ws->marks[0]) {
+    cudaSetDevice(ws->device);
+    for (auto& m : ws->marks) {
+      cudaError_t e = cudaEventCreate(&m);
+      if (e != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    }
+  }
+  ws->profiling = enable != 0;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t capacity) {
+  if (!ws || !stage_ms)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  if (!ws->profiling)
+    return fail(CLUE_ERR_RUNTIME, "profiling is not enabled on this workspace");
+  clue_status s = wait_run(ws);
+  if (s != CLUE_OK)
+    return s;
+  for (int i = 0; i < kStages && i < capacity; ++i) {
+    cudaError_t e = cudaEventElapsedTime(&stage_ms[i], ws->marks[i], ws->marks[i + 1]);
+    if (e != cudaSuccess)
+      return fail_cuda(e, "cudaEventElapsedTime");
+  }
   return CLUE_OK;
 }
 

@@ -25,6 +25,8 @@ struct clue_workspace {
   cudaEvent_t staging_event = nullptr;
   cudaEvent_t run_event = nullptr;
   RunInfo* info = nullptr;  // pinned
+  bool profiling = false;
+  cudaEvent_t marks[clue_impl::kStages + 1] = {};
   bool has_run = false;
   int64_t last_n = 0;
   std::vector<clue_impl::EventDesc> last_events;

@@ -105,8 +105,12 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t n_events, int32_t gr
 size_t scratch_bytes(const RunShape& s, bool sigma, bool unc, bool tags);
 
 // Enqueues the whole run on `stream`. Tables must already be on the device.
+// When `marks` is not null it holds kStages + 1 events recorded at the stage
+// boundaries (extents | tiles | gather | density | nearest higher | labels).
+constexpr int kStages = 6;
 cudaError_t launch_run(const RunShape& shape, const RunParams& prm, const RunIO& io,
-                       const DeviceBuffers& b, cudaStream_t stream);
+                       const DeviceBuffers& b, cudaStream_t stream,
+                       cudaEvent_t* marks = nullptr);
 
 // Device -> host helpers used after a run.
 cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, int32_t* offsets,

@@ -500,7 +500,7 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
 
 cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io,
-                       const DeviceBuffers& b, cudaStream_t st) {
+                       const DeviceBuffers& b, cudaStream_t st, cudaEvent_t* marks) {
   const int D = sh.D;
   const int64_t n = sh.n;
   CoordPtrs x{}, sig{};
@@ -515,8 +515,14 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
       return e_;                  \
   } while (0)
 #define CLUE_LAUNCHED() CLUE_CHECK(cudaGetLastError())
+#define CLUE_MARK(i)                             \
+  do {                                           \
+    if (marks)                                   \
+      CLUE_CHECK(cudaEventRecord(marks[i], st)); \
+  } while (0)
 
   // grid extents
+  CLUE_MARK(0);
   k_grid_init<<<(sh.n_grids * kMaxDim + 127) / 128, 128, 0, st>>>(b.grid_minmax, sh.n_grids);
   CLUE_LAUNCHED();
   k_minmax<<<sh.n_chunks, kThreads, 0, st>>>(D, x, b.chunks, b.events, b.grid_minmax);
@@ -525,6 +531,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   CLUE_LAUNCHED();
 
   // counting sort by tile
+  CLUE_MARK(1);
   CLUE_CHECK(cudaMemsetAsync(b.tile_count, 0, sizeof(int32_t) * sh.n_tiles, st));
   k_bin<<<sh.n_chunks, kThreads, 0, st>>>(prm, x, b.chunks, b.events, b.grids, b.tile_of,
                                            b.point_event, b.tile_count);
@@ -544,6 +551,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   k_tile_merge_copy<<<148, kThreads, 0, st>>>(b.tile_offset, b.oversize, b.counters + 2,
                                               b.merge_tmp, b.perm);
   CLUE_LAUNCHED();
+  CLUE_MARK(2);
   k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
                                              io.unc, io.tags, b.point_event, b.sorted_coords,
                                              b.sorted_weight, b.sorted_sigma, b.sorted_unc,
@@ -568,8 +576,11 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.out_nh = io.nh ? io.nh : b.nh;
   a.out_seed = io.is_seed;
   a.seed_flag = b.seed_flag;
+  CLUE_MARK(3);
   CLUE_CHECK(launch_density(D, prm, a, st));
+  CLUE_MARK(4);
   CLUE_CHECK(launch_nearest_higher(D, prm, a, st));
+  CLUE_MARK(5);
 
   // seeds and labels
   CLUE_CHECK(scan(b.seed_flag, b.seed_rank, n, b.counters + 1, b, st));
@@ -578,6 +589,8 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.seed_flag, b.seed_rank, b.point_event,
                                              io.cluster_index, b.seeds, b.seed_event, b.status);
   CLUE_LAUNCHED();
+  CLUE_MARK(6);
+#undef CLUE_MARK
 #undef CLUE_LAUNCHED
 #undef CLUE_CHECK
   return cudaSuccess;

@@ -142,6 +142,15 @@ clue_status clue_workspace_bytes(const clue_workspace* ws, size_t* bytes);
 /* Device bytes a run over n points / n_tiles tiles would need (admission). */
 size_t clue_workspace_bytes_for(int32_t ndim, int64_t n_points, int64_t n_tiles, int32_t n_events);
 
+/* Stage timing (off by default): when enabled, every run records CUDA events at
+ * its stage boundaries on the run's stream. clue_workspace_stage_ms waits for
+ * the last run and returns the device time of each stage in this order:
+ * extents, tiles (bin + scan + scatter + order), gather, density,
+ * nearest_higher, labels. Profiling tools are not needed for these numbers. */
+#define CLUE_N_STAGES 6
+clue_status clue_workspace_set_profiling(clue_workspace* ws, int32_t enable);
+clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t capacity);
+
 /* ---- clustering ----------------------------------------------------------- */
 /* Clusterer::make_clusters(Queue&, PointsDevice&, metric, kernel)
  * (core/detail/Clusterer.hpp:139-151). Device pointers; asynchronous. */
