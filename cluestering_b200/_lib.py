@@ -104,6 +104,7 @@ SIGNATURES = {
         C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P, C.c_int32, C.c_int32, _P]),
     "clue_make_clusters_batched_host": (
         C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P, C.c_int32, C.c_int32, _P]),
+    "clue_make_clusters_device_noalloc": (C.c_int, [C.POINTER(Params), C.POINTER(Points), _P, _P]),
     "clue_n_clusters": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "clue_get_seeds": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "clue_get_clusters_device": (C.c_int, [_P, _P, _P, _P]),

@@ -206,6 +206,8 @@ size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
 
 }  // namespace
 
+size_t carve_buffers(DeviceBuffers* b, const Capacity& c, char* base) { return place(b, c, base); }
+
 size_t scratch_bytes(const RunShape& s, bool sigma, bool unc, bool tags) {
   Capacity c;
   c.points = s.n;

@@ -50,5 +50,9 @@ clue_status stage_inputs(clue_workspace* ws, const clue_points* h, clue_points* 
 clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st);
 clue_status wait_run(clue_workspace* ws);
 float sqrt_threshold(float r);
+RunParams make_run_params(const clue_params* p, const clue_points* pts);
+// Lays the buffers of capacity `c` out from `base` (or only measures them when
+// base is null) and returns the bytes they span.
+size_t carve_buffers(DeviceBuffers* b, const Capacity& c, char* base);
 
 }  // namespace clue_impl

@@ -177,6 +177,29 @@ clue_status clue_make_clusters_batched_host(clue_workspace* ws, const clue_param
                                             const uint32_t* event_sizes, int32_t n_events,
                                             int32_t grid_mode, void* stream);
 
+/* Single-event clustering that allocates nothing. No counterpart in the
+ * reference: it exists for callers that must not allocate device memory when
+ * they cluster, such as a framework that hands all device memory to its own
+ * caching allocator, or a real-time trigger loop with a fixed memory
+ * reservation where an allocation could fail or stall. Inputs and outputs are
+ * the caller's device buffers (as in clue_make_clusters_device); all scratch
+ * comes from one array of CLUE_NOALLOC_SCRATCH_BYTES that the library reserves
+ * in device memory on every GPU that loads it, for the life of the process.
+ *   - At most CLUE_NOALLOC_MAX_POINTS points per call; larger events are
+ *     rejected with CLUE_ERR_INVALID_ARGUMENT before any GPU work.
+ *   - The first call on a device looks up that device's copy of the array;
+ *     make it before capturing any stream.
+ *   - All calls share the array: calls whose GPU work overlaps (different
+ *     streams, or different host threads, on one device) race and corrupt each
+ *     other. Serialise them, e.g. on one stream.
+ *   - Asynchronous on `stream`. `device_status` (device pointer, may be NULL)
+ *     receives the run's status word: 0, or nonzero when a bounded wait
+ *     inside a kernel gave up. */
+#define CLUE_NOALLOC_MAX_POINTS 16384
+#define CLUE_NOALLOC_SCRATCH_BYTES (3u << 20)
+clue_status clue_make_clusters_device_noalloc(const clue_params* params, const clue_points* points,
+                                              uint32_t* device_status, void* stream);
+
 /* ---- results of the last run ---------------------------------------------- */
 /* Number of clusters (= seeds) of the last run; waits for it to finish.
  * PointsHost::n_clusters / PointsDevice::n_clusters

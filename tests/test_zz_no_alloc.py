@@ -1,0 +1,71 @@
+"""The entry point that allocates nothing, checked against the regular one.
+
+clue_make_clusters_device_noalloc is for callers that may not allocate device
+memory while they cluster (a framework whose caching allocator owns all device
+memory, a real-time loop with a fixed reservation). It takes its scratch from
+one array the library reserves on each GPU, so two calls in a row must not see
+each other's leftovers. This file is collected last so that a failure here
+leaves every other test already run.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import cluestering_b200 as clue
+from cluestering_b200 import _lib as L
+from cluestering_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+MAX_POINTS = 16384
+
+
+def _device_points(ev, torch):
+    dev = torch.device("cuda", 0)
+    return clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev))
+
+
+def _outputs(p):
+    return [p.rho.cpu().numpy().view(np.int32), p.nearest_higher.cpu().numpy(),
+            p.is_seed.cpu().numpy(), p.cluster_index.cpu().numpy()]
+
+
+def _noalloc(algo, p, stream, status):
+    prm = algo.params()
+    pts = clue.api._points_struct(p)
+    return L.load().clue_make_clusters_device_noalloc(C.byref(prm), C.byref(pts), status.data_ptr(),
+                                                      stream.cuda_stream)
+
+
+def test_noalloc_matches_the_workspace_path_on_two_calls_in_a_row():
+    torch = pytest.importorskip("torch")
+    stream = torch.cuda.Stream()
+    status = torch.full((1,), 123, dtype=torch.int32, device="cuda")
+    # Two different events, the second smaller: stale scratch from the first
+    # call would show up in the second.
+    events = [(W.single_2d(MAX_POINTS, seed=71), (1.5, 5.0, 1.5)),
+              (W.blobs(5000, 8, 0.0, 60.0, 1.0, 0.1, seed=72, weights="exponential"), (1.5, 3.0, 2.0))]
+    for ev, prm in events:
+        ref = _device_points(ev, torch)
+        algo = clue.Clusterer(*prm)
+        algo.make_clusters(ref)
+        got = _device_points(ev, torch)
+        rc = _noalloc(algo, got, stream, status)
+        assert rc == L.OK, L.load().clue_last_error()
+        stream.synchronize()
+        assert int(status.item()) == 0
+        for a, b in zip(_outputs(got), _outputs(ref)):
+            assert np.array_equal(a, b)
+
+
+def test_noalloc_rejects_events_above_the_limit():
+    torch = pytest.importorskip("torch")
+    ev = W.single_2d(MAX_POINTS + 1, seed=73)
+    p = _device_points(ev, torch)
+    algo = clue.Clusterer(1.5, 5.0, 1.5)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = _noalloc(algo, p, torch.cuda.current_stream(), status)
+    assert rc == L.ERR_INVALID_ARGUMENT
+    assert b"at most 16384 points" in L.load().clue_last_error()
