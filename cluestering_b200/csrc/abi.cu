@@ -181,6 +181,13 @@ size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
   CLUE_PLACE(sorted_weight, float, N);
   CLUE_PLACE(sorted_rho, float, N);
   CLUE_PLACE(merge_tmp, int32_t, N);
+  CLUE_PLACE(work_dens, int32_t, N);
+  CLUE_PLACE(work_nh, int32_t, N);
+  CLUE_PLACE(cls_dens, int32_t, N);
+  CLUE_PLACE(cls_nh, int32_t, N);
+  CLUE_PLACE(rec_dens, float4, N);
+  CLUE_PLACE(rec_nh, float4, N);
+  CLUE_PLACE(rec_tag, uint32_t, N);
   CLUE_PLACE(seeds, int32_t, N);
   CLUE_PLACE(seed_event, int32_t, N);
   CLUE_PLACE(scan_desc, unsigned long long, c.scan_blocks);

@@ -40,6 +40,14 @@ struct DeviceBuffers {
   uint32_t* sorted_tag = nullptr;
   float* sorted_rho = nullptr;
   int32_t* merge_tmp = nullptr;
+  // sweep processing order and packed candidate records
+  int32_t* work_dens = nullptr;
+  int32_t* work_nh = nullptr;
+  int32_t* cls_dens = nullptr;
+  int32_t* cls_nh = nullptr;
+  float4* rec_dens = nullptr;
+  float4* rec_nh = nullptr;
+  uint32_t* rec_tag = nullptr;
   // seeds
   int32_t* seeds = nullptr;
   int32_t* seed_event = nullptr;

@@ -561,6 +561,14 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   // the two sweeps
   SweepArgs a{};
   a.n = n;
+  a.n_tiles = sh.n_tiles;
+  a.work_dens = b.work_dens;
+  a.work_nh = b.work_nh;
+  a.cls_dens = b.cls_dens;
+  a.cls_nh = b.cls_nh;
+  a.rec_dens = b.rec_dens;
+  a.rec_nh = b.rec_nh;
+  a.rec_tag = b.rec_tag;
   a.events = b.events;
   a.grids = b.grids;
   a.tile_offset = b.tile_offset;
@@ -576,6 +584,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.out_nh = io.nh ? io.nh : b.nh;
   a.out_seed = io.is_seed;
   a.seed_flag = b.seed_flag;
+  CLUE_CHECK(launch_work_order(D, prm, a, st));
   CLUE_MARK(3);
   CLUE_CHECK(launch_density(D, prm, a, st));
   CLUE_MARK(4);

@@ -9,6 +9,12 @@
 // search box in the same order, so every rho is bit-identical to the serial
 // result. The nearest-higher choice is order-independent given identical rho and
 // distances (the comparisons form a strict order on (distance, rho, tag)).
+//
+// Warp-uniform work. The thread -> point assignment is free: each sweep
+// processes points in an order where the points of one tile are grouped by the
+// shape of their search box (launch_work_order). The 32 lanes of a warp then
+// walk the same tiles and read the same candidate at the same time, so every
+// candidate load is one broadcast and the loops do not diverge.
 #include <cfloat>
 
 #include "sweep.cuh"
@@ -69,19 +75,142 @@ __device__ __forceinline__ int tile_id(const GridDesc& g, const RunParams& p, in
 }
 
 template <int D>
+__device__ __forceinline__ void load_point(const RunParams& p, const SweepArgs& a, int64_t s, float* x,
+                                           float* sg) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    x[d] = a.sx[d * a.n + s];
+    sg[d] = ((p.has_sigma >> d) & 1) ? a.ssig[d * a.n + s] : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Work order: within each tile, points grouped by search-box class
+// ---------------------------------------------------------------------------
+
+template <int D>
+__host__ __device__ constexpr int box_classes() {
+  return D == 1 ? 9 : D == 2 ? 81 : D == 3 ? 729 : 1;
+}
+
+// Class of a search box relative to the point's own tile: per dimension
+// (own - inf, sup - own) each capped at 2, so points of one tile with equal
+// class have equal boxes whenever the box spans at most 3 tiles per dimension.
+template <int D>
+__device__ __forceinline__ int box_class(const GridDesc& g, const int* own, const int* inf,
+                                         const int* sup) {
+  if (box_classes<D>() == 1)
+    return 0;
+  int c = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const int lo = min(max(own[d] - inf[d], 0), 2);
+    const int hi = min(max(sup[d] - own[d], 0), 2);
+    c = c * 9 + lo * 3 + hi;
+  }
+  return c;
+}
+
+// Exclusive scan of cnt[0..E) in place by one warp.
+template <int E>
+__device__ void warp_scan_counts(int* cnt) {
+  const int lane = threadIdx.x & 31;
+  constexpr int per = (E + 31) / 32;
+  int local[per];
+  int sum = 0;
+#pragma unroll
+  for (int j = 0; j < per; ++j) {
+    const int k = lane * per + j;
+    local[j] = k < E ? cnt[k] : 0;
+    sum += local[j];
+  }
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o)
+      incl += y;
+  }
+  int run = incl - sum;
+#pragma unroll
+  for (int j = 0; j < per; ++j) {
+    const int k = lane * per + j;
+    if (k < E)
+      cnt[k] = run;
+    run += local[j];
+  }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_work_order(const RunParams p, const SweepArgs a) {
+  constexpr int E = box_classes<D>();
+  __shared__ int cnt[2][E];
+  for (int64_t t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+    const int begin = a.tile_offset[t], end = a.tile_offset[t + 1];
+    if (end - begin == 0)
+      continue;
+    if (end - begin == 1 || E == 1) {
+      for (int s = begin + threadIdx.x; s < end; s += blockDim.x) {
+        a.work_dens[s] = s;
+        a.work_nh[s] = s;
+      }
+      continue;
+    }
+    for (int i = threadIdx.x; i < 2 * E; i += blockDim.x)
+      (&cnt[0][0])[i] = 0;
+    __syncthreads();
+    const EventDesc ev = a.events[a.sevt[begin]];
+    const GridDesc& g = a.grids[ev.grid];
+    int own[D];
+    {
+      int local = (int)t - ev.tile_base;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        own[d] = local / g.stride[d];
+        local -= own[d] * g.stride[d];
+      }
+    }
+    for (int s = begin + threadIdx.x; s < end; s += blockDim.x) {
+      float xi[D], si[D];
+      load_point<D>(p, a, s, xi, si);
+      int inf[D], sup[D];
+      search_box<D>(g, p, xi, si, p.dc, inf, sup);
+      const int cd = box_class<D>(g, own, inf, sup);
+      search_box<D>(g, p, xi, si, p.dm, inf, sup);
+      const int cn = box_class<D>(g, own, inf, sup);
+      a.cls_dens[s] = cd;
+      a.cls_nh[s] = cn;
+      atomicAdd(&cnt[0][cd], 1);
+      atomicAdd(&cnt[1][cn], 1);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    if (warp < 2)
+      warp_scan_counts<E>(cnt[warp]);
+    __syncthreads();
+    for (int s = begin + threadIdx.x; s < end; s += blockDim.x) {
+      a.work_dens[begin + atomicAdd(&cnt[0][a.cls_dens[s]], 1)] = s;
+      a.work_nh[begin + atomicAdd(&cnt[1][a.cls_nh[s]], 1)] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Generic sweeps: any D, metric, kernel and option
+// ---------------------------------------------------------------------------
+
+template <int D>
 __global__ void __launch_bounds__(kThreads) k_density(const RunParams p, const SweepArgs a) {
   const int64_t n = a.n;
   const bool mahalanobis = p.metric_kind == CLUE_METRIC_MAHALANOBIS;
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-       s += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int s = a.work_dens[w];
     const EventDesc ev = a.events[a.sevt[s]];
     const GridDesc& g = a.grids[ev.grid];
     float xi[D], si[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      xi[d] = a.sx[d * n + s];
-      si[d] = ((p.has_sigma >> d) & 1) ? a.ssig[d * n + s] : 0.0f;
-    }
+    load_point<D>(p, a, s, xi, si);
     const int gi = a.perm[s];
     int inf[D], sup[D], b[D];
     search_box<D>(g, p, xi, si, p.dc, inf, sup);
@@ -116,16 +245,13 @@ template <int D>
 __global__ void __launch_bounds__(kThreads) k_nearest_higher(const RunParams p, const SweepArgs a) {
   const int64_t n = a.n;
   const bool mahalanobis = p.metric_kind == CLUE_METRIC_MAHALANOBIS;
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-       s += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int s = a.work_nh[w];
     const EventDesc ev = a.events[a.sevt[s]];
     const GridDesc& g = a.grids[ev.grid];
     float xi[D], si[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      xi[d] = a.sx[d * n + s];
-      si[d] = ((p.has_sigma >> d) & 1) ? a.ssig[d * n + s] : 0.0f;
-    }
+    load_point<D>(p, a, s, xi, si);
     const int gi = a.perm[s];
     const float rho_i = a.srho[s];
     const float unc = p.has_unc ? a.sunc[s] : 1.0f;
@@ -182,27 +308,220 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher(const RunParams p, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fast path: D = 2 or 3, Euclidean, no sigma, no wrapped coordinate.
+// Candidates are packed float4 records; `sqrt(d2) <= r` is tested as
+// `d2 <= thr` with the exact threshold computed on the host; the tiles of one
+// row of the search box (last dimension) are contiguous and read as one range.
+// ---------------------------------------------------------------------------
+
+template <int D>
+__device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
+  // meta::accumulate right fold: dx^2 + (dy^2 [+ dz^2])
+  const float dx = __fsub_rn(xi[0], r.x), dy = __fsub_rn(xi[1], r.y);
+  if (D == 2)
+    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float dz = __fsub_rn(xi[2], r.z);
+  return __fadd_rn(__fmul_rn(dx, dx), __fadd_rn(__fmul_rn(dy, dy), __fmul_rn(dz, dz)));
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_pack_density(const RunParams p, const SweepArgs a) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const float w = a.sw[s];
+    // flat: contribution of a neighbour is fl(flat * w_j) (ConvolutionalKernel.hpp:24-27)
+    const float v = p.kernel_kind == CLUE_KERNEL_FLAT ? __fmul_rn(p.kernel_p0, w) : w;
+    float4 r;
+    r.x = a.sx[s];
+    r.y = a.sx[a.n + s];
+    if (D == 2) {
+      r.z = v;
+      r.w = w;
+    } else {
+      r.z = a.sx[2 * a.n + s];
+      r.w = v;
+    }
+    a.rec_dens[s] = r;
+  }
+}
+
+// Row iteration shared by both fast sweeps: calls body(q) for every candidate
+// of the search box in the reference's order.
+template <int D, typename Body>
+__device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const GridDesc& g, int base,
+                                                   const int* inf, const int* sup, Body&& body) {
+  if (D == 2) {
+    for (int b0 = inf[0]; b0 <= sup[0]; ++b0) {
+      const int row = base + b0 * g.stride[0];
+      const int qe = a.tile_offset[row + sup[1] + 1];
+      for (int q = a.tile_offset[row + inf[1]]; q < qe; ++q)
+        body(q);
+    }
+  } else {
+    for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
+      for (int b1 = inf[1]; b1 <= sup[1]; ++b1) {
+        const int row = base + b0 * g.stride[0] + b1 * g.stride[1];
+        const int qe = a.tile_offset[row + sup[2] + 1];
+        for (int q = a.tile_offset[row + inf[2]]; q < qe; ++q)
+          body(q);
+      }
+  }
+}
+
+template <int D, int KIND>
+__global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, const SweepArgs a) {
+  const int64_t n = a.n;
+  const float4* __restrict__ rec = a.rec_dens;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int s = a.work_dens[w];
+    const EventDesc ev = a.events[a.sevt[s]];
+    const GridDesc& g = a.grids[ev.grid];
+    const float4 ri = rec[s];
+    const float xi[3] = {ri.x, ri.y, ri.z};
+    const float zero[3] = {0.0f, 0.0f, 0.0f};
+    const float wi = a.sw[s];
+    int inf[D], sup[D];
+    search_box<D>(g, p, xi, zero, p.dc, inf, sup);
+    float rho = 0.0f;
+    for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
+      const float4 r = __ldg(&rec[q]);
+      const float d2 = sq_dist<D>(xi, r);
+      if (d2 <= p.dc2) {
+        const float v = D == 2 ? r.z : r.w;
+        if (KIND == CLUE_KERNEL_FLAT) {
+          rho = __fadd_rn(rho, q == s ? wi : v);
+        } else {
+          const float k = kernel_value(p, __fsqrt_rn(d2), q == s);
+          rho = __fadd_rn(rho, __fmul_rn(k, v));
+        }
+      }
+    });
+    a.srho[s] = rho;
+    const int gi = a.perm[s];
+    if (a.out_rho)
+      a.out_rho[gi] = rho;
+    const uint32_t tag = p.has_tags ? a.stag[s] : (uint32_t)gi;
+    if (D == 2) {
+      a.rec_nh[s] = make_float4(xi[0], xi[1], rho, __uint_as_float(tag));
+    } else {
+      a.rec_nh[s] = make_float4(xi[0], xi[1], xi[2], rho);
+      a.rec_tag[s] = tag;
+    }
+  }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParams p,
+                                                                  const SweepArgs a) {
+  const int64_t n = a.n;
+  const float4* __restrict__ rec = a.rec_nh;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int s = a.work_nh[w];
+    const EventDesc ev = a.events[a.sevt[s]];
+    const GridDesc& g = a.grids[ev.grid];
+    const float4 ri = rec[s];
+    const float xi[3] = {ri.x, ri.y, ri.z};
+    const float zero[3] = {0.0f, 0.0f, 0.0f};
+    const float rho_i = D == 2 ? ri.z : ri.w;
+    const uint32_t tag_i = D == 2 ? __float_as_uint(ri.w) : a.rec_tag[s];
+    const float unc = p.has_unc ? a.sunc[s] : 1.0f;
+    const float min_density = __fmul_rn(p.rhoc, unc);
+    const bool seedlike = rho_i >= min_density;  // ClusteringKernels.hpp:168
+    const float eff2 = seedlike ? p.seed2 : p.dm2;
+    // rho_j == rho_i && rho_j > 0 is rho_j == rho_i && rho_i > 0
+    const bool tie_ok = rho_i > 0.0f;
+    int inf[D], sup[D];
+    search_box<D>(g, p, xi, zero, p.dm, inf, sup);
+    float delta = FLT_MAX;
+    int best = -1;
+    float rho_b = 0.0f;
+    uint32_t tag_b = 0;
+    for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
+      const float4 r = __ldg(&rec[q]);
+      const float rho_j = D == 2 ? r.z : r.w;
+      const uint32_t tag_j = D == 2 ? __float_as_uint(r.w) : __ldg(&a.rec_tag[q]);
+      const bool higher = (rho_j > rho_i) || ((rho_j == rho_i) && tie_ok && (tag_j > tag_i));
+      const float d2 = sq_dist<D>(xi, r);
+      if (higher && d2 <= eff2) {
+        const float dist = __fsqrt_rn(d2);
+        if ((dist < delta) || ((dist == delta) && (best >= 0) &&
+                               ((rho_j > rho_b) || ((rho_j == rho_b) && (tag_j > tag_b))))) {
+          delta = dist;
+          best = q;
+          rho_b = rho_j;
+          tag_b = tag_j;
+        }
+      }
+    });
+    const int gi = a.perm[s];
+    const int nh = best >= 0 ? a.perm[best] : -1;
+    a.out_nh[gi] = nh;
+    const int seed = (nh == -1) && seedlike;
+    a.seed_flag[gi] = seed;
+    if (a.out_seed)
+      a.out_seed[gi] = seed;
+  }
+}
 
 }  // namespace
 
-#define CLUE_DISPATCH_D(D, KERNEL, ...)                                         \
-  switch (D) {                                                                 \
-    case 1: KERNEL<1><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 2: KERNEL<2><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 3: KERNEL<3><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 4: KERNEL<4><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 5: KERNEL<5><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 6: KERNEL<6><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 7: KERNEL<7><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 8: KERNEL<8><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 9: KERNEL<9><<<__VA_ARGS__>>>(p, a); break;                           \
-    case 10: KERNEL<10><<<__VA_ARGS__>>>(p, a); break;                         \
-    default: return cudaErrorInvalidValue;                                     \
+bool sweep_fast_path(const RunParams& p) {
+  if ((p.D != 2 && p.D != 3) || p.metric_kind != CLUE_METRIC_EUCLIDEAN || p.has_sigma)
+    return false;
+  for (int d = 0; d < p.D; ++d)
+    if (p.wrapped[d])
+      return false;
+  return true;
+}
+
+#define CLUE_DISPATCH_D(D, KERNEL, ...)                \
+  switch (D) {                                        \
+    case 1: KERNEL<1><<<__VA_ARGS__>>>(p, a); break;  \
+    case 2: KERNEL<2><<<__VA_ARGS__>>>(p, a); break;  \
+    case 3: KERNEL<3><<<__VA_ARGS__>>>(p, a); break;  \
+    case 4: KERNEL<4><<<__VA_ARGS__>>>(p, a); break;  \
+    case 5: KERNEL<5><<<__VA_ARGS__>>>(p, a); break;  \
+    case 6: KERNEL<6><<<__VA_ARGS__>>>(p, a); break;  \
+    case 7: KERNEL<7><<<__VA_ARGS__>>>(p, a); break;  \
+    case 8: KERNEL<8><<<__VA_ARGS__>>>(p, a); break;  \
+    case 9: KERNEL<9><<<__VA_ARGS__>>>(p, a); break;  \
+    case 10: KERNEL<10><<<__VA_ARGS__>>>(p, a); break; \
+    default: return cudaErrorInvalidValue;            \
   }
+
+cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
+  if (a.n == 0)
+    return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>(a.n_tiles, 148 * 16);
+  CLUE_DISPATCH_D(D, k_work_order, blocks, kThreads, 0, st)
+  return cudaGetLastError();
+}
+
+template <int D>
+cudaError_t launch_density_fast(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
+  k_pack_density<D><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+  switch (p.kernel_kind) {
+    case CLUE_KERNEL_FLAT:
+      k_density_fast<D, CLUE_KERNEL_FLAT><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      break;
+    case CLUE_KERNEL_GAUSSIAN:
+      k_density_fast<D, CLUE_KERNEL_GAUSSIAN><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      break;
+    default:
+      k_density_fast<D, CLUE_KERNEL_EXPONENTIAL><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      break;
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launch_density(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   if (a.n == 0)
     return cudaSuccess;
+  if (sweep_fast_path(p))
+    return D == 2 ? launch_density_fast<2>(p, a, st) : launch_density_fast<3>(p, a, st);
   CLUE_DISPATCH_D(D, k_density, grid_for(a.n), kThreads, 0, st)
   return cudaGetLastError();
 }
@@ -210,6 +529,13 @@ cudaError_t launch_density(int D, const RunParams& p, const SweepArgs& a, cudaSt
 cudaError_t launch_nearest_higher(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   if (a.n == 0)
     return cudaSuccess;
+  if (sweep_fast_path(p)) {
+    if (D == 2)
+      k_nearest_higher_fast<2><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+    else
+      k_nearest_higher_fast<3><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+    return cudaGetLastError();
+  }
   CLUE_DISPATCH_D(D, k_nearest_higher, grid_for(a.n), kThreads, 0, st)
   return cudaGetLastError();
 }
