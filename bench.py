@@ -166,7 +166,7 @@ def run_reference(args, world, rank):
     from cluestering_b200 import workloads as W
     if rank != 0:
         return 0
-    ev, sizes = W.batch_2d()
+    ev, sizes = W.batch_2d(n_events=args.events)
     threads = os.cpu_count() or 1
     budget = args.cpu_sample_points
     for _ in range(args.warmup):
@@ -202,7 +202,7 @@ def run_ours(args, world, rank, local):
     hbm_peak, peak_kind = measured_peaks()
 
     # ---- workload, resident in HBM --------------------------------------------------------------
-    ev, sizes = W.batch_2d(seed=3 + 1000 * rank)
+    ev, sizes = W.batch_2d(n_events=args.events, seed=3 + 1000 * rank)
     n_total = int(sizes.sum())
     coords_d = torch.from_numpy(ev.coords).to(dev)
     weights_d = torch.from_numpy(ev.weights).to(dev)
@@ -363,6 +363,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-points", type=int, default=3_000_000)
     ap.add_argument("--plain-events", type=int, default=4096)
+    ap.add_argument("--events", type=int, default=4096,
+                    help="events per batch (4096 is the benchmark; fewer only for profiling)")
     ap.add_argument("--skip-extras", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

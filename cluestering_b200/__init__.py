@@ -17,6 +17,7 @@ from .api import (  # noqa: F401
     PeriodicEuclideanMetric,
     PointsDevice,
     PointsHost,
+    Server,
     WeightedChebyshevMetric,
     WeightedEuclideanMetric,
     clusters_csr,

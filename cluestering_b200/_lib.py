@@ -60,10 +60,13 @@ class Points(C.Structure):
     ]
 
 
+class ServerProfile(C.Structure):
+    _fields_ = [("ndim", C.c_int32), ("params", Params)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [
         ("device", C.c_int32),
-        ("ndim", C.c_int32),
         ("budget_bytes", C.c_size_t),
         ("max_inflight", C.c_int32),
         ("max_batch_events", C.c_int32),
@@ -117,8 +120,9 @@ SIGNATURES = {
     "clue_host_malloc_pinned": (C.c_int, [C.POINTER(_P), C.c_size_t]),
     "clue_host_free_pinned": (C.c_int, [_P]),
     "clue_memcpy_async": (C.c_int, [_P, _P, C.c_size_t, C.c_int32, _P]),
-    "clue_server_create": (C.c_int, [C.POINTER(_P), C.POINTER(ServerConfig), C.POINTER(Params)]),
-    "clue_server_submit": (C.c_int, [_P, C.POINTER(Points), C.POINTER(C.c_uint64)]),
+    "clue_server_create": (
+        C.c_int, [C.POINTER(_P), C.POINTER(ServerConfig), C.POINTER(ServerProfile), C.c_int32]),
+    "clue_server_submit": (C.c_int, [_P, C.c_int32, C.POINTER(Points), C.POINTER(C.c_uint64)]),
     "clue_server_poll": (C.c_int, [_P, C.c_uint64]),
     "clue_server_drain": (C.c_int, [_P]),
     "clue_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),

@@ -409,3 +409,78 @@ class Clusterer:
         b = C.c_size_t()
         L.check(L.load().clue_workspace_bytes(self._workspace(), C.byref(b)))
         return b.value
+
+
+# ---------------------------------------------------------------------------
+# Serving (continuous batching; no counterpart in the reference)
+# ---------------------------------------------------------------------------
+
+
+class Server:
+    """Request loop over clue_server_*: submit events as they arrive, poll or drain.
+
+    `profiles` is a list of (ndim, Clusterer, metric, kernel) describing the
+    kinds of events the server accepts; submit() names the profile by index.
+    The host arrays of a submitted event must stay alive and unmodified until
+    it completes (pinned arrays are copied by DMA).
+    """
+
+    def __init__(self, profiles, *, device: int = 0, budget_bytes: int = 8 << 30, max_inflight: int = 4,
+                 max_batch_events: int = 1024, max_batch_points: int = 0, linger_us: int = 200):
+        lib = L.load()
+        arr = (L.ServerProfile * len(profiles))()
+        for i, (ndim, clusterer, metric, kernel) in enumerate(profiles):
+            arr[i].ndim = ndim
+            arr[i].params = clusterer.params(metric, kernel)
+        cfg = L.ServerConfig(device=device, budget_bytes=budget_bytes, max_inflight=max_inflight,
+                             max_batch_events=max_batch_events, max_batch_points=max_batch_points,
+                             linger_us=linger_us)
+        h = C.c_void_p()
+        L.check(lib.clue_server_create(C.byref(h), C.byref(cfg), arr, len(profiles)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, profile: int, points: PointsHost) -> int:
+        s = _points_struct(points)
+        t = C.c_uint64()
+        L.check(L.load().clue_server_submit(self._h, profile, C.byref(s), C.byref(t)))
+        self._keep[t.value] = points
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        st = L.load().clue_server_poll(self._h, ticket)
+        if st == L.ERR_NOT_READY:
+            return False
+        L.check(st)
+        self._keep.pop(ticket, None)
+        return True
+
+    def drain(self) -> None:
+        L.check(L.load().clue_server_drain(self._h))
+        self._keep.clear()
+
+    def stats(self) -> dict:
+        s = L.ServerStats()
+        L.check(L.load().clue_server_stats_get(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in L.ServerStats._fields_}
+
+    def latencies_ms(self) -> np.ndarray:
+        n = C.c_int64()
+        L.check(L.load().clue_server_latencies(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float64)
+        L.check(L.load().clue_server_latencies(self._h, out.ctypes.data, n.value, C.byref(n)))
+        return out[: n.value]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            L.load().clue_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -120,6 +120,12 @@ cudaError_t launch_run(const RunShape& shape, const RunParams& prm, const RunIO&
                        const DeviceBuffers& b, cudaStream_t stream,
                        cudaEvent_t* marks = nullptr);
 
+// Turns the batch-wide results of a run into per-event results: cluster ids
+// restart at 0 in every event and nearest-higher ids become event-local, which
+// is exactly what each event gets when clustered alone.
+cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
+                            int32_t* cluster_index, int32_t* nh, cudaStream_t stream);
+
 // Device -> host helpers used after a run.
 cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, int32_t* offsets,
                                 int32_t* points, int32_t n_clusters_upper, cudaStream_t stream);

@@ -475,6 +475,21 @@ __global__ void k_labels(int64_t n, int32_t* parent, const int32_t* seed_flag,
   }
 }
 
+// Per-event relabelling after a batched run with one grid per event.
+__global__ void k_localize(const EventDesc* events, const int32_t* point_event,
+                           const int32_t* seed_rank, int64_t n, int32_t* cluster_index,
+                           int32_t* nh) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const EventDesc ev = events[point_event[i]];
+    const int c = cluster_index[i];
+    if (c >= 0)
+      cluster_index[i] = c - seed_rank[ev.begin];
+    if (nh && nh[i] >= 0)
+      nh[i] -= ev.begin;
+  }
+}
+
 int grid_for(int64_t n, int per_block = kThreads) {
   const int64_t b = (n + per_block - 1) / per_block;
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
@@ -498,6 +513,16 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
 }  // namespace
 
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
+
+cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
+                            int32_t* cluster_index, int32_t* nh, cudaStream_t st) {
+  (void)n_events;
+  if (n == 0)
+    return cudaSuccess;
+  k_localize<<<grid_for(n), kThreads, 0, st>>>(b.events, b.point_event, b.seed_rank, n,
+                                              cluster_index, nh);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io,
                        const DeviceBuffers& b, cudaStream_t st, cudaEvent_t* marks) {

@@ -315,6 +315,18 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher(const RunParams p, 
 // row of the search box (last dimension) are contiguous and read as one range.
 // ---------------------------------------------------------------------------
 
+// Order-preserving image of a density: key(a) > key(b) iff a > b and equal
+// densities give equal keys. NaN maps to 0, below every number, so a NaN
+// density is never "higher" (every comparison with NaN is false). Densities
+// are never -0 (they start at +0 and round-to-nearest sums of opposite values
+// give +0), so no other pair of equal values has different keys.
+__device__ __forceinline__ uint32_t rho_key(float rho) {
+  if (rho != rho)
+    return 0u;
+  const uint32_t b = __float_as_uint(rho);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
 template <int D>
 __device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
   // meta::accumulate right fold: dx^2 + (dy^2 [+ dz^2])
@@ -355,6 +367,7 @@ __device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const Gri
     for (int b0 = inf[0]; b0 <= sup[0]; ++b0) {
       const int row = base + b0 * g.stride[0];
       const int qe = a.tile_offset[row + sup[1] + 1];
+#pragma unroll 4
       for (int q = a.tile_offset[row + inf[1]]; q < qe; ++q)
         body(q);
     }
@@ -363,6 +376,7 @@ __device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const Gri
       for (int b1 = inf[1]; b1 <= sup[1]; ++b1) {
         const int row = base + b0 * g.stride[0] + b1 * g.stride[1];
         const int qe = a.tile_offset[row + sup[2] + 1];
+#pragma unroll 4
         for (int q = a.tile_offset[row + inf[2]]; q < qe; ++q)
           body(q);
       }
@@ -403,15 +417,44 @@ __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, co
     if (a.out_rho)
       a.out_rho[gi] = rho;
     const uint32_t tag = p.has_tags ? a.stag[s] : (uint32_t)gi;
+    const float key = __uint_as_float(rho_key(rho));
     if (D == 2) {
-      a.rec_nh[s] = make_float4(xi[0], xi[1], rho, __uint_as_float(tag));
+      a.rec_nh[s] = make_float4(xi[0], xi[1], key, __uint_as_float(tag));
     } else {
-      a.rec_nh[s] = make_float4(xi[0], xi[1], xi[2], rho);
+      a.rec_nh[s] = make_float4(xi[0], xi[1], xi[2], key);
       a.rec_tag[s] = tag;
     }
   }
 }
 
+__device__ __forceinline__ float next_up(float x) {  // x >= 0, finite
+  return __uint_as_float(__float_as_uint(x) + 1u);
+}
+__device__ __forceinline__ float next_down(float x) {  // x >= 0; next_down(0) = -denorm_min
+  return x > 0.0f ? __uint_as_float(__float_as_uint(x) - 1u) : __uint_as_float(0x80000001u);
+}
+
+// Squared distances that bracket the rounding class of `delta` (a correctly
+// rounded square root): every d2 <= lo has sqrt_rn(d2) < delta and every
+// d2 >= hi has sqrt_rn(d2) > delta. With a = the float below delta,
+// lo = next_down(fl(a*a)) <= a^2 and, with b = the float above, hi =
+// next_up(fl(b*b)) >= b^2; sqrt_rn is monotone, which gives both claims.
+__device__ __forceinline__ void bracket(float delta, float& lo, float& hi) {
+  const float a = next_down(delta);
+  lo = next_down(__fmul_rn(a, a));
+  const float b = next_up(delta);
+  const float bb = __fmul_rn(b, b);
+  hi = isinf(bb) ? bb : next_up(bb);
+}
+
+// Nearest higher with (density, tag) as one ordered 64-bit key and distances
+// compared as squared distances. A candidate j of point i is eligible when it is
+// "higher" (key_j > key_i, which is rho_j > rho_i, or equal densities above zero
+// and tag_j > tag_i) and sqrt(d2) <= the effective distance (d2 <= eff2). Against
+// the current best (distance delta) it wins when sqrt(d2) < delta, or when
+// sqrt(d2) == delta and key_j > key_best (ClusteringKernels.hpp:195-202). The
+// bracket decides all but the candidates whose squared distance falls in
+// (lo, hi); those take the exact square root.
 template <int D>
 __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParams p,
                                                                   const SweepArgs a) {
@@ -425,35 +468,45 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
     const float4 ri = rec[s];
     const float xi[3] = {ri.x, ri.y, ri.z};
     const float zero[3] = {0.0f, 0.0f, 0.0f};
-    const float rho_i = D == 2 ? ri.z : ri.w;
+    const float rho_i = a.srho[s];
     const uint32_t tag_i = D == 2 ? __float_as_uint(ri.w) : a.rec_tag[s];
     const float unc = p.has_unc ? a.sunc[s] : 1.0f;
     const float min_density = __fmul_rn(p.rhoc, unc);
     const bool seedlike = rho_i >= min_density;  // ClusteringKernels.hpp:168
     const float eff2 = seedlike ? p.seed2 : p.dm2;
-    // rho_j == rho_i && rho_j > 0 is rho_j == rho_i && rho_i > 0
-    const bool tie_ok = rho_i > 0.0f;
+    // rho_j == rho_i && rho_j > 0 && tag_j > tag_i: with rho_i <= 0 (or NaN)
+    // equal densities never count, so the tag part of the key is saturated.
+    const bool nan_i = rho_i != rho_i;
+    const uint64_t key_i =
+        ((uint64_t)(nan_i ? 0xffffffffu : rho_key(rho_i)) << 32) |
+        ((nan_i || !(rho_i > 0.0f)) ? 0xffffffffu : tag_i);
     int inf[D], sup[D];
     search_box<D>(g, p, xi, zero, p.dm, inf, sup);
     float delta = FLT_MAX;
+    float lo = __int_as_float(0x7f800000), hi = lo;  // no best yet: every eligible wins
     int best = -1;
-    float rho_b = 0.0f;
-    uint32_t tag_b = 0;
+    uint64_t key_b = 0;
     for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
       const float4 r = __ldg(&rec[q]);
-      const float rho_j = D == 2 ? r.z : r.w;
       const uint32_t tag_j = D == 2 ? __float_as_uint(r.w) : __ldg(&a.rec_tag[q]);
-      const bool higher = (rho_j > rho_i) || ((rho_j == rho_i) && tie_ok && (tag_j > tag_i));
+      const uint64_t key_j = ((uint64_t)__float_as_uint(D == 2 ? r.z : r.w) << 32) | tag_j;
       const float d2 = sq_dist<D>(xi, r);
-      if (higher && d2 <= eff2) {
+      const bool cand = (key_j > key_i) && (d2 <= eff2);
+      const bool clear = cand && (d2 <= lo);
+      if (cand && !clear && d2 < hi) {
+        // rounding class of delta: decide exactly
         const float dist = __fsqrt_rn(d2);
-        if ((dist < delta) || ((dist == delta) && (best >= 0) &&
-                               ((rho_j > rho_b) || ((rho_j == rho_b) && (tag_j > tag_b))))) {
+        if ((dist < delta) || ((dist == delta) && (best >= 0) && (key_j > key_b))) {
           delta = dist;
+          bracket(delta, lo, hi);
           best = q;
-          rho_b = rho_j;
-          tag_b = tag_j;
+          key_b = key_j;
         }
+      } else if (clear) {
+        delta = __fsqrt_rn(d2);
+        bracket(delta, lo, hi);
+        best = q;
+        key_b = key_j;
       }
     });
     const int gi = a.perm[s];

@@ -239,22 +239,30 @@ clue_status clue_host_free_pinned(void* ptr);
 clue_status clue_memcpy_async(void* dst, const void* src, size_t bytes, int32_t kind, void* stream);
 
 /* ---- serving -------------------------------------------------------------- */
-/* A request loop with continuous batching: events are submitted from host
- * memory as they arrive, admitted while their device footprint fits the
- * memory budget, grouped by size into batches that run concurrently on
- * several streams, and completed individually. Each event gets the
- * single-event result (CLUE_GRID_PER_EVENT semantics), so its result does not
+/* A request loop with continuous batching (no counterpart in the reference,
+ * whose callers run one make_clusters per event and thread, as in
+ * benchmark/throughput/worker.cpp:17-39). Events are submitted from host memory
+ * as they arrive. A scheduler thread groups pending events of one profile by
+ * size, admits a batch when a stream slot is free and the batch's device
+ * footprint fits the memory budget, and runs it while earlier batches are
+ * still on the GPU; each event completes on its own. Every event gets the
+ * single-event result (CLUE_GRID_PER_EVENT semantics), so a result does not
  * depend on what it was batched with. */
 typedef struct clue_server clue_server;
 
+/* Events of one profile share ndim and clustering parameters. */
+typedef struct {
+  int32_t ndim;
+  clue_params params;
+} clue_server_profile;
+
 typedef struct {
   int32_t device;
-  int32_t ndim;          /* all events of a server share ndim and params */
-  size_t budget_bytes;   /* device memory the server may hold for in-flight work */
-  int32_t max_inflight;  /* batches in flight at once (streams) */
-  int32_t max_batch_events;
-  int64_t max_batch_points;
-  int32_t linger_us;     /* how long a partial batch may wait for company */
+  size_t budget_bytes;      /* device memory the server may hold (all slots) */
+  int32_t max_inflight;     /* batches on the GPU at once (one stream each) */
+  int32_t max_batch_events; /* events per batch */
+  int64_t max_batch_points; /* points per batch (0: derived from the budget) */
+  int32_t linger_us;        /* how long a small batch may wait for company */
 } clue_server_config;
 
 typedef struct {
@@ -265,10 +273,14 @@ typedef struct {
 } clue_server_stats;
 
 clue_status clue_server_create(clue_server** server, const clue_server_config* config,
-                               const clue_params* params);
-/* Queues one event; the host buffers must stay valid until it completes.
- * Outputs land in points->cluster_index (and the optional outputs). */
-clue_status clue_server_submit(clue_server* server, const clue_points* points, uint64_t* ticket);
+                               const clue_server_profile* profiles, int32_t n_profiles);
+/* Queues one event of the given profile. The host buffers must stay valid (and
+ * unmodified) until the event completes; pinned buffers are copied by DMA,
+ * pageable ones through the server's pinned staging. Outputs land in
+ * points->cluster_index (and the optional outputs). An event larger than a
+ * batch can hold is rejected with CLUE_ERR_OUT_OF_MEMORY. */
+clue_status clue_server_submit(clue_server* server, int32_t profile, const clue_points* points,
+                               uint64_t* ticket);
 /* CLUE_OK when the event completed, CLUE_ERR_NOT_READY otherwise. */
 clue_status clue_server_poll(clue_server* server, uint64_t ticket);
 /* Waits until every submitted event has completed. */

@@ -265,6 +265,30 @@ def test_reference_datasets(name):
     check(c, w, 1.5, 10.0, 1.5)
 
 
+# ---- ties ---------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("spacing", [1.0, 0.1, 0.3])
+def test_lattice_ties_2d(spacing):
+    # Equal densities and equal distances everywhere: the tag tie-break and the
+    # equal-distance rule decide; with spacing 0.1 or 0.3 squared distances of
+    # equal true length differ only by rounding.
+    g = np.arange(70, dtype=np.float32) * np.float32(spacing)
+    xx, yy = np.meshgrid(g, g, indexing="ij")
+    coords = np.stack([xx.ravel(), yy.ravel()]).astype(np.float32)
+    w = np.ones(coords.shape[1], np.float32)
+    check(coords, w, 1.5 * spacing, 3.0, 1.5 * spacing)
+    check(coords, w, 1.01 * spacing, 2.0, 2.9 * spacing)
+
+
+def test_lattice_ties_3d_with_duplicates():
+    g = np.arange(18, dtype=np.float32) * np.float32(0.1)
+    xx, yy, zz = np.meshgrid(g, g, g, indexing="ij")
+    coords = np.stack([xx.ravel(), yy.ravel(), zz.ravel()]).astype(np.float32)
+    coords = np.concatenate([coords, coords[:, ::7]], axis=1)  # coincident copies
+    w = np.ones(coords.shape[1], np.float32)
+    check(coords, w, 0.15, 4.0, 0.25)
+
+
 # ---- edge cases ---------------------------------------------------------------------------------
 
 def test_single_point():

@@ -1,0 +1,134 @@
+"""The serving loop: every event's result is the same alone and in the mix.
+
+Events of two profiles (2-D flat kernel, 3-D Gaussian kernel) and many sizes
+are submitted while earlier batches run; each result must equal, bit for bit,
+the single-event call on that event alone.
+"""
+
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import cluestering_b200 as clue
+from cluestering_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+P2 = (2, clue.Clusterer(1.5, 5.0, 1.5), clue.EuclideanMetric(), clue.FlatKernel(0.5))
+P3 = (3, clue.Clusterer(3.0, 10.0, 4.0), clue.EuclideanMetric(), clue.GaussianKernel(1.0, 1.0))
+
+
+def _events(n, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for e in range(n):
+        size = int(np.exp(rng.uniform(np.log(300), np.log(30000))))
+        if rng.uniform() < 0.75:
+            out.append((0, W.blobs(size, max(1, round(20 * size / 16384)), 0, 100, 1.0, 0.1, seed * 1000 + e)))
+        else:
+            out.append((1, W.layered_3d(size, seed=seed * 1000 + e)))
+    return out
+
+
+def _alone(profile, ev):
+    ndim, algo, metric, kernel = (P2, P3)[profile]
+    p = clue.PointsHost(ev.coords, ev.weights)
+    p.is_seed = np.zeros(ev.n, np.int32)
+    p.rho = np.zeros(ev.n, np.float32)
+    p.nearest_higher = np.zeros(ev.n, np.int32)
+    algo.make_clusters(p, metric, kernel)
+    return p
+
+
+def _host_points(ev, pinned=False):
+    if pinned:
+        import torch
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        p = clue.PointsHost(pin(ev.coords), pin(ev.weights))
+        p.cluster_index = pin(np.full(ev.n, -7, np.int32))
+        p.is_seed = pin(np.zeros(ev.n, np.int32))
+        p.rho = pin(np.zeros(ev.n, np.float32))
+        p.nearest_higher = pin(np.zeros(ev.n, np.int32))
+        return p
+    p = clue.PointsHost(ev.coords, ev.weights)
+    p.is_seed = np.zeros(ev.n, np.int32)
+    p.rho = np.zeros(ev.n, np.float32)
+    p.nearest_higher = np.zeros(ev.n, np.int32)
+    return p
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_results_are_the_same_alone_and_in_the_mix(pinned):
+    evs = _events(60, seed=1 if pinned else 2)
+    with clue.Server([P2, P3], max_inflight=3, max_batch_events=16, budget_bytes=2 << 30,
+                     linger_us=500) as srv:
+        pts = [_host_points(ev, pinned) for _, ev in evs]
+        tickets = [srv.submit(prof, p) for (prof, _), p in zip(evs, pts)]
+        srv.drain()
+        assert all(srv.done(t) for t in tickets)
+        st = srv.stats()
+        assert st["completed"] == len(evs) and st["batches"] >= 2
+    for (prof, ev), p in zip(evs, pts):
+        a = _alone(prof, ev)
+        assert np.array_equal(p.rho.view(np.int32), a.rho.view(np.int32))
+        assert np.array_equal(p.nearest_higher, a.nearest_higher)
+        assert np.array_equal(p.is_seed, a.is_seed)
+        assert np.array_equal(p.cluster_index, a.cluster_index)
+
+
+def test_served_results_match_the_checker():
+    evs = _events(6, seed=3)
+    with clue.Server([P2, P3]) as srv:
+        pts = [_host_points(ev) for _, ev in evs]
+        for (prof, _), p in zip(evs, pts):
+            srv.submit(prof, p)
+        srv.drain()
+    for (prof, ev), p in zip(evs, pts):
+        kw = dict(kernel="flat", kernel_params=(0.5,)) if prof == 0 else \
+            dict(kernel="gaussian", kernel_params=(1.0, 1.0))
+        prm = (1.5, 5.0, 1.5) if prof == 0 else (3.0, 10.0, 4.0)
+        o = O.make_clusters(ev.coords, ev.weights, *prm, exp_mode=O.EXP_CLUE, **kw)
+        assert np.array_equal(p.cluster_index, o.cluster_index)
+        assert np.array_equal(p.nearest_higher, o.nearest_higher)
+
+
+def test_arrivals_while_batches_run():
+    evs = _events(80, seed=4)
+    pts = [_host_points(ev, pinned=True) for _, ev in evs]
+    with clue.Server([P2, P3], max_inflight=2, max_batch_events=8, linger_us=100) as srv:
+        tickets = []
+
+        def client():
+            rng = np.random.default_rng(0)
+            for (prof, _), p in zip(evs, pts):
+                tickets.append(srv.submit(prof, p))
+                time.sleep(rng.exponential(0.0005))
+
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        srv.drain()
+        lat = srv.latencies_ms()
+        st = srv.stats()
+    assert len(lat) == len(evs) and (lat > 0).all()
+    assert st["latency_p99_ms"] >= st["latency_p50_ms"] > 0
+    assert st["points_completed"] == sum(ev.n for _, ev in evs)
+    for (prof, ev), p in zip(evs, pts):
+        assert np.array_equal(p.cluster_index, _alone(prof, ev).cluster_index)
+
+
+def test_submit_rejects_what_the_server_cannot_take():
+    ev = W.single_2d(2000, seed=5)
+    with clue.Server([P2], budget_bytes=64 << 20, max_inflight=1, max_batch_events=4) as srv:
+        big = W.single_2d(3_000_000, seed=6)
+        with pytest.raises(MemoryError):
+            srv.submit(0, clue.PointsHost(big.coords, big.weights))
+        with pytest.raises(ValueError):
+            srv.submit(0, clue.PointsHost(np.vstack([ev.coords, ev.coords[:1]]), ev.weights))
+        p = clue.PointsHost(ev.coords, ev.weights)
+        p.set_tags(np.arange(ev.n))
+        with pytest.raises(ValueError):
+            srv.submit(0, p)
