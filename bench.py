@@ -261,6 +261,9 @@ def run_ours(args, world, rank, local):
     extras = {}
     if rank == 0 and not args.skip_extras:
         extras = run_extras(args, ev, sizes, local, stream, hbm_peak)
+        del coords_d, weights_d, pts
+        torch.cuda.empty_cache()
+        extras["serving"] = run_serving(args, local)
 
     if rank != 0:
         return 0
@@ -355,6 +358,78 @@ def run_extras(args, ev, sizes, local, stream, hbm_peak):
     return out
 
 
+def run_serving(args, local):
+    """Serving form on a mixed stream: saturated throughput, then Poisson
+    arrivals at fractions of it, with per-event latency (completion - arrival).
+    The plain per-event form (one synchronous call per event) runs on the same
+    stream for comparison."""
+    import torch
+
+    import cluestering_b200 as clue
+    from cluestering_b200 import workloads as W
+
+    evs = list(W.serving_mix(args.serve_events))
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    pts = []
+    for ev in evs:
+        p = clue.PointsHost(pin(ev.coords), pin(ev.weights))
+        p.cluster_index = pin(np.zeros(ev.n, np.int32))
+        pts.append(p)
+    profs = [(2, clue.Clusterer(1.5, 5.0, 1.5, device=local), clue.EuclideanMetric(), clue.FlatKernel(0.5)),
+             (3, clue.Clusterer(3.0, 10.0, 4.0, device=local), clue.EuclideanMetric(),
+              clue.GaussianKernel(1.0, 1.0))]
+    prof_of = [0 if ev.ndim == 2 else 1 for ev in evs]
+    total = sum(ev.n for ev in evs)
+    cfg = dict(device=local, budget_bytes=40 << 30, max_inflight=args.serve_inflight,
+               max_batch_events=args.serve_batch_events, max_batch_points=args.serve_batch_points,
+               linger_us=args.serve_linger_us)
+    out = {"events": len(evs), "points": total, "mix": "80% 2-D single_2d-style, 20% 3-D layered_3d-style",
+           "sizes": "log-uniform [1024, 262144]", "config": cfg}
+    with clue.Server(profs, **cfg) as srv:
+        for i in range(min(32, len(evs))):  # warm-up
+            srv.submit(prof_of[i], pts[i])
+        srv.drain()
+        t0 = time.perf_counter()
+        for i, p in enumerate(pts):
+            srv.submit(prof_of[i], p)
+        srv.drain()
+        peak = total / (time.perf_counter() - t0)
+    out["peak_points_per_s"] = peak
+    peak_events = peak / (total / len(evs))
+    loads = []
+    rng = np.random.default_rng(0)
+    for f in args.serve_loads:
+        with clue.Server(profs, **cfg) as srv:
+            gaps = rng.exponential(1.0 / (f * peak_events), size=len(evs))
+            t_next = time.perf_counter()
+            t0 = t_next
+            for i, p in enumerate(pts):
+                t_next += gaps[i]
+                while time.perf_counter() < t_next:
+                    pass
+                srv.submit(prof_of[i], p)
+            srv.drain()
+            dt = time.perf_counter() - t0
+            lat = srv.latencies_ms()
+            st = srv.stats()
+        loads.append({"load": f, "points_per_s": total / dt, "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)), "batches": st["batches"]})
+    out["loads"] = loads
+    half = min(loads, key=lambda r: abs(r["load"] - 0.5))
+    out["p50_ms_at_half_load"], out["p99_ms_at_half_load"] = half["p50_ms"], half["p99_ms"]
+    # plain per-event on the same stream
+    algos = [profs[0][1], profs[1][1]]
+    for i in range(min(16, len(evs))):
+        algos[prof_of[i]].make_clusters(pts[i], profs[prof_of[i]][2], profs[prof_of[i]][3])
+    t0 = time.perf_counter()
+    for i, p in enumerate(pts):
+        algos[prof_of[i]].make_clusters(p, profs[prof_of[i]][2], profs[prof_of[i]][3])
+    plain = total / (time.perf_counter() - t0)
+    out["plain_per_event_points_per_s"] = plain
+    out["speedup_vs_plain"] = peak / plain
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -365,6 +440,12 @@ def main():
     ap.add_argument("--plain-events", type=int, default=4096)
     ap.add_argument("--events", type=int, default=4096,
                     help="events per batch (4096 is the benchmark; fewer only for profiling)")
+    ap.add_argument("--serve-events", type=int, default=1500)
+    ap.add_argument("--serve-inflight", type=int, default=4)
+    ap.add_argument("--serve-batch-events", type=int, default=64)
+    ap.add_argument("--serve-batch-points", type=int, default=2_000_000)
+    ap.add_argument("--serve-linger-us", type=int, default=200)
+    ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--skip-extras", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
