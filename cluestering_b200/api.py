@@ -359,6 +359,7 @@ class Clusterer:
         if not host and synchronize:
             L.check(lib.clue_stream_synchronize(st))
         points.clustered = True
+        self._last_n = points.size()
         return points
 
     @staticmethod
@@ -395,6 +396,19 @@ class Clusterer:
         nk = C.c_int32()
         L.check(L.load().clue_sample_associations(self._ws, offs.ctypes.data, B + 1, C.byref(nk)))
         return offs, nk.value
+
+    def getClustersDevice(self, stream=None):  # noqa: N802
+        """Cluster -> points map of the last run built on the device:
+        (offsets, points) CUDA tensors, ids ascending within a cluster."""
+        import torch
+        k = self.n_clusters()
+        dev = torch.device("cuda", self._device)
+        offsets = torch.empty(k + 1, dtype=torch.int32, device=dev)
+        pts = torch.empty(max(1, self._last_n), dtype=torch.int32, device=dev)
+        st = self._stream_handle(stream, False)
+        L.check(L.load().clue_get_clusters_device(self._ws, offsets.data_ptr(), pts.data_ptr(), st))
+        L.check(L.load().clue_stream_synchronize(st))
+        return offsets, pts[: int(offsets[-1].item())]
 
     def set_profiling(self, enable: bool = True) -> None:
         L.check(L.load().clue_workspace_set_profiling(self._workspace(), int(enable)))

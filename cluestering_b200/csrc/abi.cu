@@ -462,6 +462,7 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   ws->has_run = true;
   ws->last_n = sh.n;
   ws->last_events = t.events;
+  ws->last_labels = pts->cluster_index;
   return CLUE_OK;
 }
 
@@ -795,11 +796,16 @@ clue_status clue_sample_associations(clue_workspace* ws, int32_t* offsets, int32
 
 clue_status clue_get_clusters_device(clue_workspace* ws, int32_t* offsets, int32_t* points,
                                      void* stream) {
-  (void)ws;
-  (void)offsets;
-  (void)points;
-  (void)stream;
-  return fail(CLUE_ERR_RUNTIME, "clue_get_clusters_device is not available in this build");
+  if (!ws || !offsets || !points)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  clue_status s = wait_run(ws);
+  if (s != CLUE_OK)
+    return s;
+  cudaError_t e = cudaSetDevice(ws->device);
+  if (e == cudaSuccess)
+    e = launch_clusters_csr(ws->b, ws->last_n, ws->last_labels, ws->info->n_seeds, offsets, points,
+                            (cudaStream_t)stream);
+  return e == cudaSuccess ? CLUE_OK : fail_cuda(e, "cluster map");
 }
 
 clue_status clue_stream_create(void** stream, int32_t device) {

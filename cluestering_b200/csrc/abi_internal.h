@@ -30,6 +30,7 @@ struct clue_workspace {
   bool has_run = false;
   int64_t last_n = 0;
   std::vector<clue_impl::EventDesc> last_events;
+  const int32_t* last_labels = nullptr;  // device cluster ids of the last run
 };
 
 namespace clue_impl {

@@ -127,8 +127,9 @@ cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
                             int32_t* cluster_index, int32_t* nh, cudaStream_t stream);
 
 // Device -> host helpers used after a run.
-cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, int32_t* offsets,
-                                int32_t* points, int32_t n_clusters_upper, cudaStream_t stream);
+cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t* labels,
+                                int32_t n_clusters, int32_t* offsets, int32_t* points,
+                                cudaStream_t stream);
 
 int scan_blocks_for(int64_t n);
 

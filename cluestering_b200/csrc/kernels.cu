@@ -289,8 +289,8 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const int32_t* tile_of, in
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n;
        base += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = base + threadIdx.x;
-    const bool valid = i < n;
-    const int t = valid ? tile_of[i] : -1;
+    const int t = i < n ? tile_of[i] : -1;
+    const bool valid = t >= 0;  // negative keys (outliers) are not placed
     const unsigned mask = __match_any_sync(kFull, t);
     const int leader = __ffs(mask) - 1;
     int pos = 0;
@@ -299,6 +299,19 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const int32_t* tile_of, in
     pos = __shfl_sync(kFull, pos, leader);
     if (valid)
       perm[pos + __popc(mask & lanemask_lt())] = (int32_t)i;
+  }
+}
+
+// Histogram of non-negative keys (warp-aggregated atomics).
+__global__ void __launch_bounds__(kThreads) k_hist(const int32_t* keys, int64_t n, int32_t* count) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    const int t = i < n ? keys[i] : -1;
+    const unsigned mask = __match_any_sync(kFull, t);
+    if (t >= 0 && lane == __ffs(mask) - 1)
+      atomicAdd(&count[t], __popc(mask));
   }
 }
 
@@ -513,6 +526,40 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
 }  // namespace
 
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
+
+// utils/detail/get_clusters.hpp:24-49 on the device: cluster -> points as CSR,
+// point ids ascending within a cluster (the order the reference's serial
+// make_associator produces). The same stable counting sort as the tile
+// binning, keyed by cluster id; outliers (-1) are left out.
+cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t* labels,
+                                int32_t n_clusters, int32_t* offsets, int32_t* points,
+                                cudaStream_t st) {
+  int32_t* count = b.parent;    // free after the run: n >= n_clusters
+  int32_t* cursor = b.tile_of;  // idem
+  cudaError_t e;
+  if (n_clusters == 0)
+    return cudaMemsetAsync(offsets, 0, sizeof(int32_t), st);
+  if ((e = cudaMemsetAsync(count, 0, sizeof(int32_t) * n_clusters, st)))
+    return e;
+  k_hist<<<grid_for(n), kThreads, 0, st>>>(labels, n, count);
+  if ((e = cudaGetLastError()))
+    return e;
+  if ((e = scan(count, offsets, n_clusters, offsets + n_clusters, b, st)))
+    return e;
+  if ((e = cudaMemcpyAsync(cursor, offsets, sizeof(int32_t) * n_clusters, cudaMemcpyDeviceToDevice, st)))
+    return e;
+  k_scatter<<<grid_for(n), kThreads, 0, st>>>(labels, n, cursor, points);
+  if ((e = cudaGetLastError()))
+    return e;
+  if ((e = cudaMemsetAsync(b.counters + 2, 0, sizeof(int32_t), st)))
+    return e;
+  k_tile_sort<<<(int)std::min<int64_t>(n_clusters, 148 * 32), kThreads, 0, st>>>(
+      offsets, n_clusters, points, b.oversize, b.counters + 2);
+  k_tile_merge<<<148, kThreads, 0, st>>>(offsets, b.oversize, b.counters + 2, points, b.merge_tmp);
+  k_tile_merge_copy<<<148, kThreads, 0, st>>>(offsets, b.oversize, b.counters + 2, b.merge_tmp,
+                                              points);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
                             int32_t* cluster_index, int32_t* nh, cudaStream_t st) {

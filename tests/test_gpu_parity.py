@@ -332,6 +332,17 @@ def test_workspace_reuse_across_sizes():
         assert_identical(g, run_oracle(ev.coords, ev.weights, 1.5, 5.0, 1.5))
 
 
+@pytest.mark.parametrize("host", [True, False])
+def test_cluster_map_built_on_the_device(host):
+    # utils/detail/get_clusters.hpp:24-49: cluster -> points, ids ascending.
+    ev = W.blobs(30000, 5, 0.0, 30.0, 1.0, 0.1, seed=50)  # clusters larger than one sort pass
+    g = run_gpu(ev.coords, ev.weights, 1.5, 5.0, 1.5, path="host" if host else "device")
+    offsets, pts = g["clusterer"].getClustersDevice()
+    ref_off, ref_pts = clue.clusters_csr(g["ci"])
+    assert np.array_equal(offsets.cpu().numpy(), ref_off)
+    assert np.array_equal(pts.cpu().numpy(), ref_pts)
+
+
 def test_host_and_device_entry_points_agree():
     ev = W.single_2d(8000, seed=7)
     a = run_gpu(ev.coords, ev.weights, 1.5, 5.0, 1.5, path="host")
