@@ -377,6 +377,22 @@ RunParams make_run_params(const clue_params* p, const clue_points* pts) {
       r.has_sigma |= 1 << d;
   r.has_unc = pts->density_uncertainty != nullptr;
   r.has_tags = pts->tags != nullptr;
+  // Gaussian denominator (2 * std) * std, rounded as the device rounds it.
+  r.gauss_inv_den = 0.0f;
+  r.exp_in_range = 0;
+  if (p->kernel_kind == CLUE_KERNEL_GAUSSIAN) {
+    const float den = (2.0f * p->kernel_params[0]) * p->kernel_params[0];
+    int e = 0;
+    const float m = std::frexp(den, &e);
+    if (m == 0.5f && e - 1 >= -125 && e - 1 <= 125)
+      r.gauss_inv_den = std::ldexp(1.0f, 1 - e);
+    // exponents of in-range pairs lie in [-(dc^2/den)(1 + 2^-22), 0]
+    r.exp_in_range = std::isfinite(den) && den > 0.0f &&
+                     (double)p->dc * (double)p->dc / (double)den <= 100.0;
+  } else if (p->kernel_kind == CLUE_KERNEL_EXPONENTIAL) {
+    // exponents lie in [-(avg * dc)(1 + 2^-23), 0]
+    r.exp_in_range = (double)p->kernel_params[0] * (double)p->dc <= 100.0;
+  }
   return r;
 }
 

@@ -64,6 +64,13 @@ struct RunParams {
   int32_t has_sigma;  // bit d set when sigma[d] is present
   int32_t has_unc;
   int32_t has_tags;
+  // Gaussian kernel: 2^-k when (2 * std) * std is the power of two 2^k, else 0.
+  // Dividing by 2^k and multiplying by 2^-k round the same exact value once,
+  // so the division can be a multiplication.
+  float gauss_inv_den;
+  // Nonzero when every exponent the kernel can see for an in-range pair
+  // (distance <= dc) lies where clue_expf needs no special-case branch.
+  int32_t exp_in_range;
 };
 
 // ---------------------------------------------------------------------------
@@ -209,6 +216,26 @@ __device__ __forceinline__ float kernel_value(const RunParams& p, float dist, bo
     default:
       return __int_as_float(0x7fc00000);
   }
+}
+
+// Kernel value of an in-range pair for the fast sweep: the same operations as
+// kernel_value, with the Gaussian division replaced by the exact power-of-two
+// multiplication when available and clue_expf's range branches dropped when the
+// host proved they cannot trigger (RunParams::exp_in_range).
+__device__ __forceinline__ float kernel_value_in_range(const RunParams& p, float dist, bool self) {
+  if (self)
+    return 1.0f;
+  if (p.kernel_kind == CLUE_KERNEL_GAUSSIAN) {
+    const float num = __fmul_rn(-dist, dist);
+    const float den = __fmul_rn(__fmul_rn(2.0f, p.kernel_p0), p.kernel_p0);
+    const float x = p.gauss_inv_den != 0.0f ? __fmul_rn(num, p.gauss_inv_den) : __fdiv_rn(num, den);
+    return __fmul_rn(p.kernel_p1, p.exp_in_range ? clue_expf_core(x) : clue_expf(x));
+  }
+  if (p.kernel_kind == CLUE_KERNEL_EXPONENTIAL) {
+    const float x = __fmul_rn(-p.kernel_p0, dist);
+    return __fmul_rn(p.kernel_p1, p.exp_in_range ? clue_expf_core(x) : clue_expf(x));
+  }
+  return p.kernel_p0;
 }
 
 // Status word bits written by kernels whose waits are bounded.

@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, co
         if (KIND == CLUE_KERNEL_FLAT) {
           rho = __fadd_rn(rho, q == s ? wi : v);
         } else {
-          const float k = kernel_value(p, __fsqrt_rn(d2), q == s);
+          const float k = kernel_value_in_range(p, __fsqrt_rn(d2), q == s);
           rho = __fadd_rn(rho, __fmul_rn(k, v));
         }
       }

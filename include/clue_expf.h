@@ -62,20 +62,12 @@ CLUE_EXPF_QUAL float clue_bits_to_float(uint32_t b) {
 /* 2^e for e in [-126, 127], built from its exponent bits (exact). */
 CLUE_EXPF_QUAL float clue_pow2i(int e) { return clue_bits_to_float((uint32_t)(e + 127) << 23); }
 
-CLUE_EXPF_QUAL float clue_expf(float x) {
-  /* ln(2^128) rounded down to float: above it the result overflows. */
-  const float overflow_at = 88.72283935546875f;
-  /* Below ln(2^-150) the exact result is under half the smallest subnormal. */
-  const float underflow_at = -103.97207641601562f;
+/* clue_expf for x in [underflow_at, overflow_at] (no NaN): the same operations
+ * without the special-case tests, so it returns the same bits there. */
+CLUE_EXPF_QUAL float clue_expf_core(float x) {
   const float log2e = 1.44269502162933349609375f;  /* 0x3fb8aa3b */
   const float ln2_hi = 0.693145751953125f;          /* 0x3f317200, 16 significant bits */
   const float ln2_lo = 1.428606765330187e-06f;      /* 0x35bfbe8e = ln2 - ln2_hi */
-  if (x != x)
-    return x;
-  if (x > overflow_at)
-    return clue_bits_to_float(0x7f800000u); /* +inf */
-  if (x < underflow_at)
-    return 0.0f;
   const float fn = CLUE_RINTF(CLUE_FMUL(x, log2e));
   /* r = (x - n*hi) - n*lo; n*hi is exact, so the first subtraction is exact too
    * (Sterbenz) for the range handled here. */
@@ -94,6 +86,20 @@ CLUE_EXPF_QUAL float clue_expf(float x) {
   const int n2 = n - n1;
   /* p * 2^n1 stays in the normal range (exact); the second scaling rounds once. */
   return CLUE_FMUL(CLUE_FMUL(p, clue_pow2i(n1)), clue_pow2i(n2));
+}
+
+CLUE_EXPF_QUAL float clue_expf(float x) {
+  /* ln(2^128) rounded down to float: above it the result overflows. */
+  const float overflow_at = 88.72283935546875f;
+  /* Below ln(2^-150) the exact result is under half the smallest subnormal. */
+  const float underflow_at = -103.97207641601562f;
+  if (x != x)
+    return x;
+  if (x > overflow_at)
+    return clue_bits_to_float(0x7f800000u); /* +inf */
+  if (x < underflow_at)
+    return 0.0f;
+  return clue_expf_core(x);
 }
 
 #endif /* CLUE_EXPF_H */
