@@ -192,6 +192,7 @@ size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
   CLUE_PLACE(seed_event, int32_t, N);
   CLUE_PLACE(scan_desc, unsigned long long, c.scan_blocks);
   CLUE_PLACE(counters, int32_t, 16);
+  CLUE_PLACE(large_tiles, int32_t, N / 256 + 1);
   CLUE_PLACE(oversize, int32_t, N / 4096 + 1);
   CLUE_PLACE(status, uint32_t, 1);
   CLUE_PLACE(sorted_sigma, float, c.sigma ? D * N : 0);

@@ -355,16 +355,154 @@ __device__ void sort_segment(int32_t* seg, int m, int* s) {
   __syncthreads();
 }
 
+// Rank sort of one segment of m <= 32 * R distinct ids by one warp: lane L
+// holds ids L, L + 32, ... in registers, `ids` holds all of them in shared
+// memory, and an id's final position is the number of ids below it.
+template <int R>
+__device__ __forceinline__ void warp_rank_sort(int32_t* seg, int m, int* ids, int lane) {
+  int v[R], r[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int i = k * 32 + lane;
+    v[k] = i < m ? ids[i] : INT_MAX;
+    r[k] = 0;
+  }
+  int j = 0;
+  for (; j + 4 <= m; j += 4) {
+    const int4 x = *reinterpret_cast<const int4*>(ids + j);
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      r[k] += (x.x < v[k]) + (x.y < v[k]) + (x.z < v[k]) + (x.w < v[k]);
+  }
+  for (; j < m; ++j) {
+    const int x = ids[j];
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+      r[k] += x < v[k];
+  }
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    if (k * 32 + lane < m)
+      seg[r[k]] = v[k];
+}
+
+// Orders the ids of every tile ascending. One warp per tile: tiles of up to
+// kWarpSortCap ids are rank-sorted by the warp with no block barrier; larger
+// tiles are listed for k_tile_sort_large. Tiles already in order (one warp of
+// the scatter placed all of them) are left as they are.
+constexpr int kWarpSortCap = 256;
 __global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offset, int64_t n_tiles,
-                                                        int32_t* perm, int32_t* oversize,
-                                                        int32_t* oversize_count) {
-  __shared__ int s[kSortCap];
-  for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+                                                        int32_t* perm, int32_t* large,
+                                                        int32_t* large_count) {
+  __shared__ __align__(16) int s_ids[kThreads / 32][kWarpSortCap];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int* ids = s_ids[warp];
+  const int64_t stride = (int64_t)gridDim.x * (kThreads / 32);
+  for (int64_t t = (int64_t)blockIdx.x * (kThreads / 32) + warp; t < n_tiles; t += stride) {
     const int begin = tile_offset[t], end = tile_offset[t + 1];
     const int m = end - begin;
     if (m <= 1)
       continue;
-    if (m <= kSortCap) {
+    if (m > kWarpSortCap) {
+      if (lane == 0)
+        large[atomicAdd(large_count, 1)] = (int32_t)t;
+      continue;
+    }
+    int unsorted = 0;
+    for (int i = lane; i < m; i += 32) {
+      const int v = perm[begin + i];
+      ids[i] = v;
+      if (i + 1 < m)
+        unsorted |= v > perm[begin + i + 1];
+    }
+    __syncwarp();
+    if (__any_sync(kFull, unsorted)) {
+      int32_t* seg = perm + begin;
+      if (m <= 64)
+        warp_rank_sort<2>(seg, m, ids, lane);
+      else if (m <= 128)
+        warp_rank_sort<4>(seg, m, ids, lane);
+      else
+        warp_rank_sort<8>(seg, m, ids, lane);
+    }
+    __syncwarp();
+  }
+}
+
+// Ascending bitonic sort of one value per lane across the warp.
+__device__ __forceinline__ int warp_bitonic(int v, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int o = __shfl_xor_sync(kFull, v, j);
+      const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+      v = keep_min ? min(v, o) : max(v, o);
+    }
+  }
+  return v;
+}
+
+// Number of entries of the ascending 32-entry run `c` below v.
+__device__ __forceinline__ int count_below(const int* c, int v) {
+  int p = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1)
+    p += (c[p + step - 1] < v) ? step : 0;
+  return p + (c[p] < v);
+}
+
+// Segments of kWarpSortCap < m <= kChunkRankCap ids: every warp sorts runs of
+// 32 ids in registers, then each id's position is its place in its own run
+// plus, for every other run, the number of ids below it (ids are distinct).
+constexpr int kChunkRankCap = 1024;
+__device__ void chunk_rank_sort(int32_t* seg, int m, int* s) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int unsorted = 0;
+  for (int i = threadIdx.x; i + 1 < m; i += kThreads)
+    unsorted |= seg[i] > seg[i + 1];
+  if (!__syncthreads_or(unsorted))
+    return;
+  const int runs = (m + 31) >> 5;
+  for (int c = warp; c < runs; c += kThreads / 32) {
+    const int i = c * 32 + lane;
+    s[i] = warp_bitonic(i < m ? seg[i] : INT_MAX, lane);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < runs * 32; i += kThreads) {
+    const int v = s[i];
+    if (v == INT_MAX)
+      continue;
+    const int own = i >> 5;
+    int rank = i & 31;
+    for (int c = 0; c < runs; ++c)
+      if (c != own)
+        rank += count_below(s + c * 32, v);
+    seg[rank] = v;
+  }
+  __syncthreads();
+}
+
+// Tiles listed by k_tile_sort (more than kWarpSortCap ids): one block each.
+// Up to kChunkRankCap ids: chunk_rank_sort; up to kSortCap: a shared-memory
+// bitonic sort; larger tiles become sorted chunks of kSortCap ids, listed for
+// k_tile_merge.
+__global__ void __launch_bounds__(kThreads) k_tile_sort_large(const int32_t* tile_offset,
+                                                              const int32_t* large,
+                                                              const int32_t* large_count,
+                                                              int32_t* perm, int32_t* oversize,
+                                                              int32_t* oversize_count) {
+  __shared__ int s[kSortCap];
+  const int count = *large_count;
+  for (int e = blockIdx.x; e < count; e += gridDim.x) {
+    const int t = large[e];
+    const int begin = tile_offset[t], end = tile_offset[t + 1];
+    const int m = end - begin;
+    if (m <= 1)
+      continue;
+    if (m <= kChunkRankCap) {
+      chunk_rank_sort(perm + begin, m, s);
+    } else if (m <= kSortCap) {
       sort_segment(perm + begin, m, s);
     } else {
       for (int c = begin; c < end; c += kSortCap)
@@ -450,22 +588,20 @@ __global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int
 // Seeds and labels: core/detail/ClusteringKernels.hpp:293-343, :419-446
 // ---------------------------------------------------------------------------
 
-__global__ void k_parent_init(int64_t n, const int32_t* nh, int32_t* parent) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    parent[i] = nh[i] < 0 ? (int32_t)i : nh[i];
-}
-
 // Root of each point's nearest-higher chain by pointer jumping with path
 // halving: every write stores an ancestor, so concurrent updates stay valid
-// and every step moves strictly up the tree.
-__global__ void k_labels(int64_t n, int32_t* parent, const int32_t* seed_flag,
+// and every step moves strictly up the tree. The tree is walked in the
+// tile-contiguous layout (`parent` holds sorted positions, a root points to
+// itself): a chain runs between neighbouring points, so its steps stay within
+// a few tiles and mostly hit cache, and the lanes of a warp, which start on
+// neighbouring points, share most of their chains.
+__global__ void k_labels(int64_t n, int32_t* parent, const int32_t* perm, const int32_t* seed_flag,
                          const int32_t* seed_rank, const int32_t* point_event,
                          int32_t* cluster_index, int32_t* seeds, int32_t* seed_event,
                          uint32_t* status) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int x = (int)i;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    int x = (int)s;
     int64_t steps = 0;
     for (;;) {
       const int px = __ldcg(&parent[x]);
@@ -480,10 +616,12 @@ __global__ void k_labels(int64_t n, int32_t* parent, const int32_t* seed_flag,
         break;
       }
     }
-    cluster_index[i] = seed_flag[x] ? seed_rank[x] : -1;
-    if (seed_flag[i]) {
-      seeds[seed_rank[i]] = (int32_t)i;
-      seed_event[seed_rank[i]] = point_event[i];
+    const int gi = perm[s];
+    const int gr = perm[x];
+    cluster_index[gi] = seed_flag[gr] ? seed_rank[gr] : -1;
+    if (seed_flag[gi]) {
+      seeds[seed_rank[gi]] = gi;
+      seed_event[seed_rank[gi]] = point_event[gi];
     }
   }
 }
@@ -523,6 +661,27 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
   return cudaGetLastError();
 }
 
+// Sorts ids[offsets[k] .. offsets[k + 1]) ascending for every segment k.
+cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* ids,
+                          const DeviceBuffers& b, cudaStream_t st) {
+  int32_t* oversize_count = b.counters + 2;
+  int32_t* large_count = b.counters + 3;
+  cudaError_t e = cudaMemsetAsync(oversize_count, 0, 2 * sizeof(int32_t), st);
+  if (e != cudaSuccess)
+    return e;
+  const int64_t warps_per_block = kThreads / 32;
+  const int blocks =
+      (int)std::max<int64_t>(1, std::min<int64_t>((n_segments + warps_per_block - 1) / warps_per_block,
+                                                  148 * 16));
+  k_tile_sort<<<blocks, kThreads, 0, st>>>(offsets, n_segments, ids, b.large_tiles, large_count);
+  k_tile_sort_large<<<148 * 8, kThreads, 0, st>>>(offsets, b.large_tiles, large_count, ids,
+                                                  b.oversize, oversize_count);
+  k_tile_merge<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, ids, b.merge_tmp);
+  k_tile_merge_copy<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, b.merge_tmp,
+                                              ids);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
@@ -551,14 +710,7 @@ cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t
   k_scatter<<<grid_for(n), kThreads, 0, st>>>(labels, n, cursor, points);
   if ((e = cudaGetLastError()))
     return e;
-  if ((e = cudaMemsetAsync(b.counters + 2, 0, sizeof(int32_t), st)))
-    return e;
-  k_tile_sort<<<(int)std::min<int64_t>(n_clusters, 148 * 32), kThreads, 0, st>>>(
-      offsets, n_clusters, points, b.oversize, b.counters + 2);
-  k_tile_merge<<<148, kThreads, 0, st>>>(offsets, b.oversize, b.counters + 2, points, b.merge_tmp);
-  k_tile_merge_copy<<<148, kThreads, 0, st>>>(offsets, b.oversize, b.counters + 2, b.merge_tmp,
-                                              points);
-  return cudaGetLastError();
+  return sort_segments(offsets, n_clusters, points, b, st);
 }
 
 cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
@@ -613,16 +765,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
                              cudaMemcpyDeviceToDevice, st));
   k_scatter<<<grid_for(n), kThreads, 0, st>>>(b.tile_of, n, b.tile_cursor, b.perm);
   CLUE_LAUNCHED();
-  CLUE_CHECK(cudaMemsetAsync(b.counters + 2, 0, sizeof(int32_t), st));
-  k_tile_sort<<<(int)std::min<int64_t>(sh.n_tiles, 148 * 32), kThreads, 0, st>>>(
-      b.tile_offset, sh.n_tiles, b.perm, b.oversize, b.counters + 2);
-  CLUE_LAUNCHED();
-  k_tile_merge<<<148, kThreads, 0, st>>>(b.tile_offset, b.oversize, b.counters + 2, b.perm,
-                                         b.merge_tmp);
-  CLUE_LAUNCHED();
-  k_tile_merge_copy<<<148, kThreads, 0, st>>>(b.tile_offset, b.oversize, b.counters + 2,
-                                              b.merge_tmp, b.perm);
-  CLUE_LAUNCHED();
+  CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st));
   CLUE_MARK(2);
   k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
                                              io.unc, io.tags, b.point_event, b.sorted_coords,
@@ -656,6 +799,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.out_nh = io.nh ? io.nh : b.nh;
   a.out_seed = io.is_seed;
   a.seed_flag = b.seed_flag;
+  a.parent = b.parent;
   CLUE_CHECK(launch_work_order(D, prm, a, st));
   CLUE_MARK(3);
   CLUE_CHECK(launch_density(D, prm, a, st));
@@ -665,10 +809,9 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // seeds and labels
   CLUE_CHECK(scan(b.seed_flag, b.seed_rank, n, b.counters + 1, b, st));
-  k_parent_init<<<grid_for(n), kThreads, 0, st>>>(n, a.out_nh, b.parent);
-  CLUE_LAUNCHED();
-  k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.seed_flag, b.seed_rank, b.point_event,
-                                             io.cluster_index, b.seeds, b.seed_event, b.status);
+  k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.perm, b.seed_flag, b.seed_rank,
+                                             b.point_event, io.cluster_index, b.seeds,
+                                             b.seed_event, b.status);
   CLUE_LAUNCHED();
   CLUE_MARK(6);
 #undef CLUE_MARK

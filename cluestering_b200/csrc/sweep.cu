@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher(const RunParams p, 
     for (int d = 0; d < D; ++d)
       b[d] = inf[d];
     float delta = FLT_MAX;
-    int nh = -1;
+    int nh = -1, nh_pos = s;
     float rho_nh = 0.0f;
     uint32_t tag_nh = 0;
     do {
@@ -294,12 +294,14 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher(const RunParams p, 
               ((rho_j > rho_nh) || ((rho_j == rho_nh) && (tag_j > tag_nh)))))) {
           delta = dist;
           nh = gj;
+          nh_pos = q;
           rho_nh = rho_j;
           tag_nh = tag_j;
         }
       }
     } while (next_tile<D>(b, inf, sup));
     a.out_nh[gi] = nh;
+    a.parent[s] = nh_pos;
     // KernelFindClusters, ClusteringKernels.hpp:301-313
     const int seed = (nh == -1) && (rho_i >= min_density);
     a.seed_flag[gi] = seed;
@@ -512,6 +514,7 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
     const int gi = a.perm[s];
     const int nh = best >= 0 ? a.perm[best] : -1;
     a.out_nh[gi] = nh;
+    a.parent[s] = best >= 0 ? best : s;
     const int seed = (nh == -1) && seedlike;
     a.seed_flag[gi] = seed;
     if (a.out_seed)

@@ -36,6 +36,9 @@ struct SweepArgs {
   int32_t* out_nh;     // required
   int32_t* out_seed;   // may be null
   int32_t* seed_flag;  // required
+  // Nearest higher as a sorted position (the point itself when it has none):
+  // the follower tree in the tile-contiguous layout, where chains stay local.
+  int32_t* parent;
 };
 
 // True when the packed fast path applies: D = 2 or 3, Euclidean metric, no
