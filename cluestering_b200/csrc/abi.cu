@@ -188,6 +188,14 @@ size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
   CLUE_PLACE(rec_dens, float4, N);
   CLUE_PLACE(rec_nh, float4, N);
   CLUE_PLACE(rec_tag, uint32_t, N);
+  // cell layout of 2-D and 3-D runs, sized for D = 3
+  CLUE_PLACE(nh_pos, int32_t, c.cells ? N : 0);
+  CLUE_PLACE(nh_q, int32_t, c.cells ? N : 0);
+  CLUE_PLACE(cell_slot, int32_t, c.cells ? N : 0);
+  CLUE_PLACE(cell_s, int32_t, c.cells ? T : 0);
+  CLUE_PLACE(cell_geom, float4, c.cells ? 2 * T : 0);
+  CLUE_PLACE(cell_info, CellInfo, c.cells ? N : 0);
+  CLUE_PLACE(cell_box, float4, c.cells ? 2 * N : 0);
   CLUE_PLACE(seeds, int32_t, N);
   CLUE_PLACE(seed_event, int32_t, N);
   CLUE_PLACE(scan_desc, unsigned long long, c.scan_blocks);
@@ -228,6 +236,7 @@ size_t scratch_bytes(const RunShape& s, bool sigma, bool unc, bool tags) {
   c.sigma = sigma;
   c.unc = unc;
   c.tags = tags;
+  c.cells = s.D == 2 || s.D == 3;
   DeviceBuffers b;
   return place(&b, c, nullptr);
 }
@@ -236,10 +245,12 @@ clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, b
                             int64_t staged) {
   Capacity& c = ws->cap;
   const int64_t scan_blocks = scan_blocks_for(std::max<int64_t>(s.n, s.n_tiles));
+  const bool cells = s.D == 2 || s.D == 3;
   const bool fits = c.points >= s.n && c.tiles >= s.n_tiles && c.events >= s.n_events &&
                     c.chunks >= s.n_chunks && c.grids >= s.n_grids &&
                     c.scan_blocks >= scan_blocks && c.dims >= s.D && (!sigma || c.sigma) &&
-                    (!unc || c.unc) && (!tags || c.tags) && c.staged_points >= staged;
+                    (!unc || c.unc) && (!tags || c.tags) && (!cells || c.cells) &&
+                    c.staged_points >= staged;
   if (fits)
     return CLUE_OK;
   // Grow every dimension that is short by 25 % headroom; keep what fits.
@@ -255,6 +266,7 @@ clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, b
   n.sigma = c.sigma || sigma;
   n.unc = c.unc || unc;
   n.tags = c.tags || tags;
+  n.cells = c.cells || cells;
   n.staged_points = staged ? grow(c.staged_points, staged) : c.staged_points;
   DeviceBuffers nb;
   const size_t bytes = place(&nb, n, nullptr);
@@ -370,8 +382,12 @@ RunParams make_run_params(const clue_params* p, const clue_points* pts) {
   r.kernel_p1 = p->kernel_params[1];
   r.metric_kind = p->metric_kind;
   r.dc2 = sqrt_threshold(p->dc);
-  r.dm2 = sqrt_threshold(p->dm);
-  r.seed2 = sqrt_threshold(p->seed_dc);
+  // Nearest-higher thresholds stop at FLT_MAX: the reference's search starts
+  // from delta = FLT_MAX and only takes dist < delta, so a candidate at an
+  // infinite distance (d2 = inf) never becomes the nearest higher, while every
+  // finite d2 has sqrt(d2) < FLT_MAX.
+  r.dm2 = std::min(sqrt_threshold(p->dm), FLT_MAX);
+  r.seed2 = std::min(sqrt_threshold(p->seed_dc), FLT_MAX);
   r.has_sigma = 0;
   for (int d = 0; d < pts->ndim; ++d)
     if (pts->sigma[d])

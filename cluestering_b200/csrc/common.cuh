@@ -48,6 +48,13 @@ struct Chunk {
   int32_t end;
 };
 
+// One cell of the nearest-higher layout: its members occupy [start, end) of
+// the layout, and maxkey is the largest (density, tag) key among them.
+struct alignas(16) CellInfo {
+  int32_t start, end;
+  unsigned long long maxkey;
+};
+
 // Scalar parameters of a run, passed by value to kernels.
 struct RunParams {
   int32_t D;

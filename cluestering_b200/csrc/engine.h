@@ -48,6 +48,14 @@ struct DeviceBuffers {
   float4* rec_dens = nullptr;
   float4* rec_nh = nullptr;
   uint32_t* rec_tag = nullptr;
+  // cell layout of the nearest-higher search (D = 2 or 3)
+  int32_t* nh_pos = nullptr;
+  int32_t* nh_q = nullptr;
+  int32_t* cell_slot = nullptr;
+  int32_t* cell_s = nullptr;       // per tile
+  float4* cell_geom = nullptr;     // 2 per tile
+  CellInfo* cell_info = nullptr;   // per sorted position (slot)
+  float4* cell_box = nullptr;      // 2 per slot
   // seeds
   int32_t* seeds = nullptr;
   int32_t* seed_event = nullptr;
@@ -73,6 +81,7 @@ struct Capacity {
   int64_t points = 0, tiles = 0, events = 0, chunks = 0, grids = 0, scan_blocks = 0;
   int32_t dims = 0;
   bool sigma = false, unc = false, tags = false;
+  bool cells = false;  // cell layout of the nearest-higher search (2-D and 3-D runs)
   int64_t staged_points = 0;
 };
 

@@ -800,6 +800,15 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.out_seed = io.is_seed;
   a.seed_flag = b.seed_flag;
   a.parent = b.parent;
+  if (sweep_cells_path(prm)) {
+    a.nh_pos = b.nh_pos;
+    a.nh_q = b.nh_q;
+    a.cell_slot = b.cell_slot;
+    a.cell_s = b.cell_s;
+    a.cell_geom = b.cell_geom;
+    a.cell_info = b.cell_info;
+    a.cell_box = b.cell_box;
+  }
   CLUE_CHECK(launch_work_order(D, prm, a, st));
   CLUE_MARK(3);
   CLUE_CHECK(launch_density(D, prm, a, st));

@@ -111,6 +111,7 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   cap.sigma = any_sigma;
   cap.unc = pts->density_uncertainty != nullptr;
   cap.tags = pts->tags != nullptr;
+  cap.cells = D == 2 || D == 3;
   DeviceBuffers b;
   if (carve_buffers(&b, cap, nullptr) > CLUE_NOALLOC_SCRATCH_BYTES)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "event does not fit the no-allocation scratch");

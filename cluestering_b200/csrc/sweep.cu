@@ -419,12 +419,18 @@ __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, co
     if (a.out_rho)
       a.out_rho[gi] = rho;
     const uint32_t tag = p.has_tags ? a.stag[s] : (uint32_t)gi;
-    const float key = __uint_as_float(rho_key(rho));
+    const uint32_t kbits = rho_key(rho);
+    const float key = __uint_as_float(kbits);
+    int pos = s;
+    if (a.nh_pos) {
+      pos = a.nh_pos[s];
+      atomicMax(&a.cell_info[a.cell_slot[s]].maxkey, ((unsigned long long)kbits << 32) | tag);
+    }
     if (D == 2) {
-      a.rec_nh[s] = make_float4(xi[0], xi[1], key, __uint_as_float(tag));
+      a.rec_nh[pos] = make_float4(xi[0], xi[1], key, __uint_as_float(tag));
     } else {
-      a.rec_nh[s] = make_float4(xi[0], xi[1], xi[2], key);
-      a.rec_tag[s] = tag;
+      a.rec_nh[pos] = make_float4(xi[0], xi[1], xi[2], key);
+      a.rec_tag[pos] = tag;
     }
   }
 }
@@ -522,6 +528,347 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
   }
 }
 
+// ---------------------------------------------------------------------------
+// Cell layout of the nearest-higher search (fast path without user tags).
+//
+// Every tile of m points is split into s^D cells, s the largest value with
+// s^D * kCellTarget <= m (at least 1, at most kCellDimMax). A point's cell
+// comes from cell_coord, which is monotone in the coordinate; the search
+// therefore finds every point of [a, b] in the cells cell_coord(a) ..
+// cell_coord(b), whatever rounding placed it there. Each cell records the
+// bounding box of its members and their largest key, and a cell is skipped
+// when its box is provably out of reach or none of its keys is higher.
+// ---------------------------------------------------------------------------
+
+constexpr int kCellTarget = 8;     // average points per cell
+constexpr int kCellSlots = 256;    // cells per tile at most (16^2, 6^3)
+constexpr int kCellWarps = 4;      // warps per block of k_cells
+
+template <int D>
+__host__ __device__ constexpr int cell_dim_max() {
+  return D == 2 ? 16 : 6;
+}
+
+template <int D>
+__device__ __forceinline__ int cells_per_dim(int m) {
+  int s = 1;
+  while (s < cell_dim_max<D>()) {
+    const int u = s + 1;
+    const int vol = D == 2 ? u * u : u * u * u;
+    if (vol * kCellTarget > m)
+      break;
+    s = u;
+  }
+  return s;
+}
+
+// Cell coordinate of x in a tile with origin lo and inverse cell width inv
+// (0 for a degenerate tile): monotone non-decreasing in x for every non-NaN x,
+// clamped to [0, s); NaN lands in cell 0.
+__device__ __forceinline__ int cell_coord(float x, float lo, float inv, int s) {
+  float u = __fmul_rn(__fsub_rn(x, lo), inv);
+  u = fminf(fmaxf(u, 0.0f), (float)(s - 1));
+  return (int)u;
+}
+
+// Origin and inverse cell width of the tiles' cells, dimension d.
+__device__ __forceinline__ void cell_axis(const GridDesc& g, int b, int s, int d, float& lo,
+                                          float& inv) {
+  lo = __fadd_rn(g.minv[d], __fmul_rn((float)b, g.tile[d]));
+  const float v = __fdiv_rn((float)s, g.tile[d]);
+  inv = (g.tile[d] > 0.0f && v < INFINITY) ? v : 0.0f;
+}
+
+template <int D>
+__device__ __forceinline__ void load_geom(const SweepArgs& a, int t, float* lo, float* inv) {
+  const float4 g0 = a.cell_geom[D == 2 ? t : 2 * t];
+  if (D == 2) {
+    lo[0] = g0.x, lo[1] = g0.y, inv[0] = g0.z, inv[1] = g0.w;
+  } else {
+    const float4 g1 = a.cell_geom[2 * t + 1];
+    lo[0] = g0.x, lo[1] = g0.y, lo[D - 1] = g0.z, inv[0] = g0.w, inv[1] = g1.x, inv[D - 1] = g1.y;
+  }
+}
+
+// One warp per tile: cell of every point, cell ranges and member boxes, and
+// the layout positions (a counting sort by cell inside the tile's range).
+template <int D>
+__global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a) {
+  __shared__ int s_cnt[kCellWarps][kCellSlots];
+  __shared__ int s_box[kCellWarps][kCellSlots * 2 * D];  // ordered ints: min planes, then max
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int* cnt = s_cnt[warp];
+  int* box = s_box[warp];
+  const int64_t n = a.n;
+  const int64_t stride = (int64_t)gridDim.x * kCellWarps;
+  for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
+    const int begin = a.tile_offset[t], end = a.tile_offset[t + 1];
+    const int m = end - begin;
+    if (m == 0)
+      continue;
+    const EventDesc ev = a.events[a.sevt[begin]];
+    const GridDesc& g = a.grids[ev.grid];
+    const int s = cells_per_dim<D>(m);
+    float lo[D], inv[D];
+    {
+      int local = (int)t - ev.tile_base;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int b = local / g.stride[d];
+        local -= b * g.stride[d];
+        cell_axis(g, b, s, d, lo[d], inv[d]);
+      }
+    }
+    if (lane == 0) {
+      a.cell_s[t] = s;
+      if (D == 2) {
+        a.cell_geom[t] = make_float4(lo[0], lo[1], inv[0], inv[1]);
+      } else {
+        a.cell_geom[2 * t] = make_float4(lo[0], lo[1], lo[D - 1], inv[0]);
+        a.cell_geom[2 * t + 1] = make_float4(inv[1], inv[D - 1], 0.0f, 0.0f);
+      }
+    }
+    for (int c = lane; c < kCellSlots; c += 32) {
+      cnt[c] = 0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        box[d * kCellSlots + c] = INT_MAX;
+        box[(D + d) * kCellSlots + c] = INT_MIN;
+      }
+    }
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) {
+      const int q = begin + i;
+      int c = 0;
+      bool finite_box = true;
+      float x[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        x[d] = a.sx[d * n + q];
+        c = c * s + cell_coord(x[d], lo[d], inv[d], s);
+        finite_box &= x[d] == x[d];
+      }
+      atomicAdd(&cnt[c], 1);
+      if (finite_box) {  // a point with a NaN coordinate is never within reach
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          atomicMin(&box[d * kCellSlots + c], f2ord(x[d]));
+          atomicMax(&box[(D + d) * kCellSlots + c], f2ord(x[d]));
+        }
+      }
+      a.cell_slot[q] = begin + c;
+    }
+    __syncwarp();
+    warp_scan_counts<kCellSlots>(cnt);
+    __syncwarp();
+    const int S = D == 2 ? s * s : s * s * s;
+    for (int c = lane; c < S; c += 32) {
+      CellInfo ci;
+      ci.start = begin + cnt[c];
+      ci.end = begin + (c + 1 < kCellSlots ? cnt[c + 1] : m);
+      ci.maxkey = 0ull;
+      a.cell_info[begin + c] = ci;
+      float mn[D], mx[D];
+      const bool empty = box[c] == INT_MAX;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        mn[d] = empty ? INFINITY : ord2f(box[d * kCellSlots + c]);
+        mx[d] = empty ? -INFINITY : ord2f(box[(D + d) * kCellSlots + c]);
+      }
+      if (D == 2) {
+        a.cell_box[begin + c] = make_float4(mn[0], mn[1], mx[0], mx[1]);
+      } else {
+        a.cell_box[2 * (begin + c)] = make_float4(mn[0], mn[1], mn[D - 1], mx[0]);
+        a.cell_box[2 * (begin + c) + 1] = make_float4(mx[1], mx[D - 1], 0.0f, 0.0f);
+      }
+    }
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) {
+      const int q = begin + i;
+      const int pos = begin + atomicAdd(&cnt[a.cell_slot[q] - begin], 1);
+      a.nh_pos[q] = pos;
+      a.nh_q[pos] = q;
+    }
+    __syncwarp();
+  }
+}
+
+// Lower bound of the squared distance from xi to any member of a cell, with
+// the operations of sq_dist: per dimension the gap to the box is at most
+// |fl(x_i - x_j)| of every member (rounding is monotone), and squares and the
+// right fold are monotone too.
+template <int D>
+__device__ __forceinline__ float box_lower_bound(const float* xi, const float* mn, const float* mx) {
+  float gap[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    gap[d] = fmaxf(fmaxf(__fsub_rn(mn[d], xi[d]), __fsub_rn(xi[d], mx[d])), 0.0f);
+  if (D == 2)
+    return __fadd_rn(__fmul_rn(gap[0], gap[0]), __fmul_rn(gap[1], gap[1]));
+  return __fadd_rn(__fmul_rn(gap[0], gap[0]),
+                   __fadd_rn(__fmul_rn(gap[1], gap[1]), __fmul_rn(gap[D - 1], gap[D - 1])));
+}
+
+// Search state of one point: best candidate so far (layout position), its
+// distance and key, and the squared-distance bracket of that distance.
+struct NhBest {
+  float delta, lo, hi;
+  int best;
+  uint64_t key_b;
+};
+
+// Tests the members of one cell unless the cell is empty, holds no higher
+// key, or its box is out of reach.
+template <int D>
+__device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const float* xi,
+                                           uint64_t key_i, float eff2, NhBest& st) {
+  const CellInfo ci = a.cell_info[slot];
+  if (ci.start == ci.end || ci.maxkey <= key_i)
+    return;
+  float mn[D], mx[D];
+  const float4 b0 = a.cell_box[D == 2 ? slot : 2 * slot];
+  if (D == 2) {
+    mn[0] = b0.x, mn[1] = b0.y, mx[0] = b0.z, mx[1] = b0.w;
+  } else {
+    const float4 b1 = a.cell_box[2 * slot + 1];
+    mn[0] = b0.x, mn[1] = b0.y, mn[D - 1] = b0.z, mx[0] = b0.w, mx[1] = b1.x, mx[D - 1] = b1.y;
+  }
+  const float lb2 = box_lower_bound<D>(xi, mn, mx);
+  if (lb2 > eff2 || lb2 >= st.hi)
+    return;
+  const float4* __restrict__ rec = a.rec_nh;
+  for (int q = ci.start; q < ci.end; ++q) {
+    const float4 r = __ldg(&rec[q]);
+    const uint32_t tag_j = D == 2 ? __float_as_uint(r.w) : __ldg(&a.rec_tag[q]);
+    const uint64_t key_j = ((uint64_t)__float_as_uint(D == 2 ? r.z : r.w) << 32) | tag_j;
+    const float d2 = sq_dist<D>(xi, r);
+    const bool cand = (key_j > key_i) && (d2 <= eff2);
+    const bool clear = cand && (d2 <= st.lo);
+    if (cand && !clear && d2 < st.hi) {
+      const float dist = __fsqrt_rn(d2);
+      if ((dist < st.delta) || ((dist == st.delta) && (st.best >= 0) && (key_j > st.key_b))) {
+        st.delta = dist;
+        bracket(dist, st.lo, st.hi);
+        st.best = q;
+        st.key_b = key_j;
+      }
+    } else if (clear) {
+      st.delta = __fsqrt_rn(d2);
+      bracket(st.delta, st.lo, st.hi);
+      st.best = q;
+      st.key_b = key_j;
+    }
+  }
+}
+
+// Nearest higher over the cell layout. Thread w takes layout position w, so a
+// warp holds neighbouring points. The own cell and its neighbours in the own
+// tile come first, which usually fixes a small delta; then every tile of the
+// reference's search box is visited, but only its cells that can hold a point
+// within the current bound. The result is the eligible candidate of least
+// distance, ties to the larger key (ClusteringKernels.hpp:195-202), as in
+// k_nearest_higher_fast, over exactly the same candidates.
+template <int D>
+__global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunParams p,
+                                                                   const SweepArgs a) {
+  const int64_t n = a.n;
+  const float4* __restrict__ rec = a.rec_nh;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int pi = (int)w;
+    const int s = a.nh_q[pi];
+    const float4 ri = rec[pi];
+    const float xi[3] = {ri.x, ri.y, ri.z};
+    const float zero[3] = {0.0f, 0.0f, 0.0f};
+    const float rho_i = a.srho[s];
+    const uint32_t tag_i = D == 2 ? __float_as_uint(ri.w) : a.rec_tag[pi];
+    const float unc = p.has_unc ? a.sunc[s] : 1.0f;
+    const float min_density = __fmul_rn(p.rhoc, unc);
+    const bool seedlike = rho_i >= min_density;  // ClusteringKernels.hpp:168
+    const float eff2 = seedlike ? p.seed2 : p.dm2;
+    const bool nan_i = rho_i != rho_i;
+    const uint64_t key_i =
+        ((uint64_t)(nan_i ? 0xffffffffu : rho_key(rho_i)) << 32) |
+        ((nan_i || !(rho_i > 0.0f)) ? 0xffffffffu : tag_i);
+    const EventDesc ev = a.events[a.sevt[s]];
+    const GridDesc& g = a.grids[ev.grid];
+    int inf[D], sup[D], own[D];
+    search_box<D>(g, p, xi, zero, p.dm, inf, sup);
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      own[d] = get_bin(g, p, xi[d], d);
+    const int t0 = tile_id<D>(g, p, ev.tile_base, own);
+
+    // no best yet: every eligible candidate wins
+    NhBest bs{FLT_MAX, __int_as_float(0x7f800000), __int_as_float(0x7f800000), -1, 0ull};
+
+    // Phase 0: the own cell and its neighbours in the own tile. Phase 1: every
+    // tile of the search box, cells within reach only, less those of phase 0.
+    // The own tile is skipped when the box leaves it out: get_bin sends a
+    // coordinate beyond the int range to bin 0 (x86 conversion), so a huge
+    // radius can give a box that misses the point's own tile.
+    int c0[D], b[D];
+    bool first = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      b[d] = inf[d];
+      c0[d] = 0;
+      first &= inf[d] <= own[d] && own[d] <= sup[d];
+    }
+    for (;;) {
+      const int t = first ? t0 : tile_id<D>(g, p, ev.tile_base, b);
+      const int base = a.tile_offset[t];
+      if (a.tile_offset[t + 1] != base) {
+        const int st = a.cell_s[t];
+        float glo[D], ginv[D];
+        load_geom<D>(a, t, glo, ginv);
+        // |x_j - x_i| <= R for every member that can still win (d2 <= bound2)
+        const float bound2 = fminf(eff2, bs.hi);
+        const float R = __fadd_ru(__fmul_ru(__fsqrt_ru(bound2), 1.000001f), 1e-19f);
+        int c_lo[D], c_hi[D], c[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          if (first) {
+            c0[d] = cell_coord(xi[d], glo[d], ginv[d], st);
+            c_lo[d] = max(c0[d] - 1, 0);
+            c_hi[d] = min(c0[d] + 1, st - 1);
+          } else {
+            c_lo[d] = cell_coord(__fsub_rd(xi[d], R), glo[d], ginv[d], st);
+            c_hi[d] = cell_coord(__fadd_ru(xi[d], R), glo[d], ginv[d], st);
+          }
+          c[d] = c_lo[d];
+        }
+        const bool own_tile = !first && t == t0;
+        do {
+          int lin = 0;
+          bool seen = own_tile;
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            lin = lin * st + c[d];
+            seen &= abs(c[d] - c0[d]) <= 1;
+          }
+          if (!seen)
+            visit_cell<D>(a, base + lin, xi, key_i, eff2, bs);
+        } while (next_tile<D>(c, c_lo, c_hi));
+      }
+      if (first)
+        first = false;
+      else if (!next_tile<D>(b, inf, sup))
+        break;
+    }
+
+    const int gi = a.perm[s];
+    const int qb = bs.best >= 0 ? a.nh_q[bs.best] : s;
+    const int nh = bs.best >= 0 ? a.perm[qb] : -1;
+    a.out_nh[gi] = nh;
+    a.parent[s] = qb;
+    const int seed = (nh == -1) && seedlike;
+    a.seed_flag[gi] = seed;
+    if (a.out_seed)
+      a.out_seed[gi] = seed;
+  }
+}
+
 }  // namespace
 
 bool sweep_fast_path(const RunParams& p) {
@@ -532,6 +879,8 @@ bool sweep_fast_path(const RunParams& p) {
       return false;
   return true;
 }
+
+bool sweep_cells_path(const RunParams& p) { return sweep_fast_path(p) && !p.has_tags; }
 
 #define CLUE_DISPATCH_D(D, KERNEL, ...)                \
   switch (D) {                                        \
@@ -553,6 +902,14 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
     return cudaSuccess;
   const int blocks = (int)std::min<int64_t>(a.n_tiles, 148 * 16);
   CLUE_DISPATCH_D(D, k_work_order, blocks, kThreads, 0, st)
+  if (a.nh_pos) {
+    const int cell_blocks =
+        (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, 148 * 32));
+    if (D == 2)
+      k_cells<2><<<cell_blocks, kCellWarps * 32, 0, st>>>(p, a);
+    else
+      k_cells<3><<<cell_blocks, kCellWarps * 32, 0, st>>>(p, a);
+  }
   return cudaGetLastError();
 }
 
@@ -585,6 +942,13 @@ cudaError_t launch_density(int D, const RunParams& p, const SweepArgs& a, cudaSt
 cudaError_t launch_nearest_higher(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   if (a.n == 0)
     return cudaSuccess;
+  if (a.nh_pos) {
+    if (D == 2)
+      k_nearest_higher_cells<2><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+    else
+      k_nearest_higher_cells<3><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+    return cudaGetLastError();
+  }
   if (sweep_fast_path(p)) {
     if (D == 2)
       k_nearest_higher_fast<2><<<grid_for(a.n), kThreads, 0, st>>>(p, a);

@@ -39,11 +39,30 @@ struct SweepArgs {
   // Nearest higher as a sorted position (the point itself when it has none):
   // the follower tree in the tile-contiguous layout, where chains stay local.
   int32_t* parent;
+  // Cell layout of the nearest-higher search (null unless sweep_cells_path):
+  // every tile is split into s^D cells (s per tile in cell_s, origin and
+  // inverse cell width per dimension in cell_geom); the points of a tile are
+  // reordered cell by cell inside the tile's range. A tile starting at sorted
+  // position b keeps its cells in slots b .. b + s^D - 1 (s^D never exceeds
+  // the tile's point count).
+  int32_t* nh_pos;        // sorted position -> layout position
+  int32_t* nh_q;          // layout position -> sorted position
+  int32_t* cell_slot;     // sorted position -> slot of its cell
+  int32_t* cell_s;        // per tile
+  float4* cell_geom;      // per tile: D = 2 {lo0, lo1, inv0, inv1}; D = 3 two entries
+  CellInfo* cell_info;    // per slot
+  float4* cell_box;       // per slot: bounding box of the members (D = 3: two entries)
 };
 
 // True when the packed fast path applies: D = 2 or 3, Euclidean metric, no
 // per-point sigma and no wrapped coordinate.
 bool sweep_fast_path(const RunParams& p);
+
+// True when the nearest-higher sweep runs over the cell layout: the fast path
+// without user tags. Keys (density, tag) are then unique, so the nearest
+// higher is the candidate of least distance, ties to the larger key, whatever
+// order the candidates are visited in.
+bool sweep_cells_path(const RunParams& p);
 
 cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st);
 cudaError_t launch_density(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st);

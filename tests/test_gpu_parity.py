@@ -313,6 +313,28 @@ def test_dense_blob_in_one_tile():
     check(coords, w, 0.05, 1.0, 0.1)
 
 
+def test_dense_blob_in_one_tile_3d():
+    # One tile holds most points: the nearest-higher search splits it into the
+    # most cells a 3-D tile gets.
+    rng = np.random.default_rng(13)
+    coords = np.concatenate([rng.normal(20, 0.1, (3, 9000)), rng.uniform(0, 40, (3, 1500))],
+                            axis=1).astype(np.float32)
+    w = rng.exponential(1.0, coords.shape[1]).astype(np.float32)
+    check(coords, w, 0.08, 2.0, 0.2, kernel="gaussian", kernel_params=(1.0, 0.05))
+
+
+def test_infinite_outlier_distance_with_far_points():
+    # dm = inf: the search box is the whole grid. Squared distances to the far
+    # points overflow to inf; a candidate at infinite distance never becomes
+    # the nearest higher (the search starts from delta = FLT_MAX).
+    ev = W.single_2d(2000, seed=11)
+    far = np.array([[3e19, -3e19, 3e19], [3e19, 3e19, -3e19]], np.float32)
+    coords = np.concatenate([ev.coords, far], axis=1)
+    w = np.concatenate([ev.weights, np.array([1.0, 1.0, 9.0], np.float32)])
+    g, o = check(coords, w, 1.5, 5.0, np.inf, 1.5)
+    assert (g["nh"][-3:] == -1).all()
+
+
 def test_no_seeds_when_rhoc_is_unreachable():
     ev = W.single_2d(3000, seed=5)
     g, o = check(ev.coords, ev.weights, 1.5, 1e9, 1.5)
