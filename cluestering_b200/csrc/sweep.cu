@@ -329,14 +329,30 @@ __device__ __forceinline__ uint32_t rho_key(float rho) {
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
+// (x_i - x_j)^2 and (y_i - y_j)^2 with one packed subtract and one packed
+// multiply (sm_100 f32x2): each half is the IEEE round-to-nearest result of
+// the scalar operation, so the values equal __fsub_rn / __fmul_rn.
+__device__ __forceinline__ void sq_diff_xy(float xi, float yi, float xj, float yj, float& sx,
+                                           float& sy) {
+  asm("{\n\t.reg .b64 a, b, d, s;\n\t"
+      "mov.b64 a, {%2, %3};\n\t"
+      "mov.b64 b, {%4, %5};\n\t"
+      "sub.rn.f32x2 d, a, b;\n\t"
+      "mul.rn.f32x2 s, d, d;\n\t"
+      "mov.b64 {%0, %1}, s;\n\t}"
+      : "=f"(sx), "=f"(sy)
+      : "f"(xi), "f"(yi), "f"(xj), "f"(yj));
+}
+
 template <int D>
 __device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
   // meta::accumulate right fold: dx^2 + (dy^2 [+ dz^2])
-  const float dx = __fsub_rn(xi[0], r.x), dy = __fsub_rn(xi[1], r.y);
+  float sx, sy;
+  sq_diff_xy(xi[0], xi[1], r.x, r.y, sx, sy);
   if (D == 2)
-    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    return __fadd_rn(sx, sy);
   const float dz = __fsub_rn(xi[2], r.z);
-  return __fadd_rn(__fmul_rn(dx, dx), __fadd_rn(__fmul_rn(dy, dy), __fmul_rn(dz, dz)));
+  return __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
 }
 
 template <int D>
@@ -540,7 +556,7 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
 // when its box is provably out of reach or none of its keys is higher.
 // ---------------------------------------------------------------------------
 
-constexpr int kCellTarget = 8;     // average points per cell
+constexpr int kCellTarget = 4;     // average points per cell
 constexpr int kCellSlots = 256;    // cells per tile at most (16^2, 6^3)
 constexpr int kCellWarps = 4;      // warps per block of k_cells
 
@@ -830,8 +846,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunP
         for (int d = 0; d < D; ++d) {
           if (first) {
             c0[d] = cell_coord(xi[d], glo[d], ginv[d], st);
-            c_lo[d] = max(c0[d] - 1, 0);
-            c_hi[d] = min(c0[d] + 1, st - 1);
+            c_lo[d] = c0[d] - 1;
+            c_hi[d] = c0[d] + 1;
           } else {
             c_lo[d] = cell_coord(__fsub_rd(xi[d], R), glo[d], ginv[d], st);
             c_hi[d] = cell_coord(__fadd_ru(xi[d], R), glo[d], ginv[d], st);
@@ -841,13 +857,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunP
         const bool own_tile = !first && t == t0;
         do {
           int lin = 0;
-          bool seen = own_tile;
+          bool seen = own_tile, valid = true;
 #pragma unroll
           for (int d = 0; d < D; ++d) {
-            lin = lin * st + c[d];
-            seen &= abs(c[d] - c0[d]) <= 1;
+            int cd = c[d];
+            if (first) {
+              // offsets -1, 0, 1 visited as 0, 1, -1: the own cell comes
+              // first and its nearest higher bounds the neighbours
+              cd = c0[d] + (cd - c0[d] + 2) % 3 - 1;
+              valid &= cd >= 0 && cd < st;
+            }
+            lin = lin * st + cd;
+            seen &= abs(cd - c0[d]) <= 1;
           }
-          if (!seen)
+          if (valid && !seen)
             visit_cell<D>(a, base + lin, xi, key_i, eff2, bs);
         } while (next_tile<D>(c, c_lo, c_hi));
       }
