@@ -401,13 +401,79 @@ __device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const Gri
   }
 }
 
+// Asynchronous 16-byte global -> shared copies (per thread, completion by
+// commit groups).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Contribution of candidate record r (sorted position q) to rho_i.
+template <int D, int KIND>
+__device__ __forceinline__ void density_add(const RunParams& p, const float* xi, const float4& r,
+                                            bool self, float wi, float& rho) {
+  const float d2 = sq_dist<D>(xi, r);
+  if (d2 <= p.dc2) {
+    const float v = D == 2 ? r.z : r.w;
+    if (KIND == CLUE_KERNEL_FLAT) {
+      rho = __fadd_rn(rho, self ? wi : v);
+    } else {
+      const float k = kernel_value_in_range(p, __fsqrt_rn(d2), self);
+      rho = __fadd_rn(rho, __fmul_rn(k, v));
+    }
+  }
+}
+
+constexpr int kRing = 4;       // chunks of 32 candidate records in flight per warp
+constexpr int kMaxRows = 32;   // rows of a search box the streamed path handles
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// Copies stream position c * 32 + lane (row table off/qa, row cursor rr) into
+// ring slot c % kRing, then closes the lane's commit group for chunk c.
+__device__ __forceinline__ void stream_issue(float4 (*ring)[32], const int* off, const int* qa,
+                                             const float4* rec, int c, int lane, int total,
+                                             int& rr) {
+  const int pp = c * 32 + lane;
+  if (pp < total) {
+    while (pp >= off[rr + 1])
+      ++rr;
+    cp_async16(&ring[c % kRing][lane], &rec[qa[rr] + (pp - off[rr])]);
+  }
+  cp_async_commit();
+}
+
+// Local density, one point per lane. When the 32 lanes of a warp share one
+// search box (the work order groups each tile's points by box), the warp
+// streams the box's candidate records through a shared-memory ring of kRing
+// chunks of 32 records, copied asynchronously kRing - 1 chunks ahead; every
+// lane reads each record from shared memory. The stream is the box's rows in
+// order, each a contiguous range of sorted positions, i.e. the reference's
+// summation order. Other warps read candidates from global memory.
 template <int D, int KIND>
 __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, const SweepArgs a) {
+  __shared__ __align__(16) float4 s_ring[kThreads / 32][kRing][32];
+  __shared__ int s_off[kThreads / 32][kMaxRows + 1];
+  __shared__ int s_qa[kThreads / 32][kMaxRows];
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_dens;
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
-       w += (int64_t)gridDim.x * blockDim.x) {
-    const int s = a.work_dens[w];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float4(*ring)[32] = s_ring[warp];
+  int* off = s_off[warp];
+  int* qa = s_qa[warp];
+  const int64_t warps_total = (int64_t)gridDim.x * (kThreads / 32);
+  for (int64_t w0 = ((int64_t)blockIdx.x * (kThreads / 32) + warp) * 32; w0 < n; w0 += warps_total * 32) {
+    const int64_t w = w0 + lane;
+    const bool active = w < n;
+    int s = active ? a.work_dens[w] : 0;
+    // idle lanes shadow lane 0 (the shuffle runs on every lane: a full-mask
+    // shuffle that only some lanes reach never completes)
+    const int s_lane0 = __shfl_sync(kFullMask, s, 0);
+    s = active ? s : s_lane0;
     const EventDesc ev = a.events[a.sevt[s]];
     const GridDesc& g = a.grids[ev.grid];
     const float4 ri = rec[s];
@@ -416,20 +482,94 @@ __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, co
     const float wi = a.sw[s];
     int inf[D], sup[D];
     search_box<D>(g, p, xi, zero, p.dc, inf, sup);
+    // one box for the whole warp?
+    bool same = __shfl_sync(kFullMask, ev.tile_base, 0) == ev.tile_base;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const int inf0 = __shfl_sync(kFullMask, inf[d], 0);
+      const int sup0 = __shfl_sync(kFullMask, sup[d], 0);
+      same &= (inf0 == inf[d]) & (sup0 == sup[d]);
+    }
+    bool ordered = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      ordered &= inf[d] <= sup[d];
+    const int n1 = D == 3 ? sup[1] - inf[1] + 1 : 1;
+    const int rows = ordered ? (sup[0] - inf[0] + 1) * n1 : 0;
     float rho = 0.0f;
-    for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
-      const float4 r = __ldg(&rec[q]);
-      const float d2 = sq_dist<D>(xi, r);
-      if (d2 <= p.dc2) {
-        const float v = D == 2 ? r.z : r.w;
-        if (KIND == CLUE_KERNEL_FLAT) {
-          rho = __fadd_rn(rho, q == s ? wi : v);
-        } else {
-          const float k = kernel_value_in_range(p, __fsqrt_rn(d2), q == s);
-          rho = __fadd_rn(rho, __fmul_rn(k, v));
+    if (__all_sync(kFullMask, same) && rows >= 1 && rows <= kMaxRows) {
+      // row table: lane r holds row r
+      int len = 0, start = 0;
+      if (lane < rows) {
+        const int b0 = inf[0] + lane / n1;
+        int row = ev.tile_base + b0 * g.stride[0];
+        if (D == 3)
+          row += (inf[1] + lane % n1) * g.stride[1];
+        start = a.tile_offset[row + inf[D - 1]];
+        len = a.tile_offset[row + sup[D - 1] + 1] - start;
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFullMask, incl, o);
+        if (lane >= o)
+          incl += y;
+      }
+      const int total = __shfl_sync(kFullMask, incl, 31);
+      if (lane < rows) {
+        off[lane] = incl - len;
+        qa[lane] = start;
+      }
+      if (lane == 0)
+        off[rows] = total;
+      __syncwarp();
+      // stream position of the point itself (its own tile is in the box unless
+      // get_bin's clamping left it out)
+      int p_self = -1;
+      {
+        int own[D];
+        bool in = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          own[d] = get_bin(g, p, xi[d], d);
+          in &= inf[d] <= own[d] && own[d] <= sup[d];
+        }
+        if (in) {
+          const int r = (own[0] - inf[0]) * n1 + (D == 3 ? own[1] - inf[1] : 0);
+          p_self = off[r] + (s - qa[r]);
         }
       }
-    });
+      const int chunks = (total + 31) >> 5;
+      int rr = 0;  // row cursor of this lane's copies
+#pragma unroll
+      for (int c = 0; c < kRing - 1; ++c)
+        stream_issue(ring, off, qa, rec, c, lane, total, rr);
+      for (int c = 0; c < chunks; ++c) {
+        stream_issue(ring, off, qa, rec, c + kRing - 1, lane, total, rr);
+        cp_async_wait<kRing - 1>();
+        __syncwarp();
+        const float4* chunk = ring[c % kRing];
+        const int cnt = min(32, total - c * 32);
+        const int base = c * 32;
+        if (cnt == 32) {
+#pragma unroll 8
+          for (int j = 0; j < 32; ++j)
+            density_add<D, KIND>(p, xi, chunk[j], base + j == p_self, wi, rho);
+        } else {
+          for (int j = 0; j < cnt; ++j)
+            density_add<D, KIND>(p, xi, chunk[j], base + j == p_self, wi, rho);
+        }
+        __syncwarp();
+      }
+      cp_async_wait<0>();
+      __syncwarp();
+    } else {
+      for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
+        density_add<D, KIND>(p, xi, __ldg(&rec[q]), q == s, wi, rho);
+      });
+    }
+    if (!active)
+      continue;
     a.srho[s] = rho;
     const int gi = a.perm[s];
     if (a.out_rho)
@@ -548,7 +688,7 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
 // Cell layout of the nearest-higher search (fast path without user tags).
 //
 // Every tile of m points is split into s^D cells, s the largest value with
-// s^D * kCellTarget <= m (at least 1, at most kCellDimMax). A point's cell
+// s^D * kCellTarget <= m (at least 1, at most cell_dim_max). A point's cell
 // comes from cell_coord, which is monotone in the coordinate; the search
 // therefore finds every point of [a, b] in the cells cell_coord(a) ..
 // cell_coord(b), whatever rounding placed it there. Each cell records the
@@ -556,13 +696,13 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
 // when its box is provably out of reach or none of its keys is higher.
 // ---------------------------------------------------------------------------
 
-constexpr int kCellTarget = 4;     // average points per cell
-constexpr int kCellSlots = 256;    // cells per tile at most (16^2, 6^3)
+constexpr int kCellTarget = 2;     // average points per cell
+constexpr int kCellSlots = 2048;   // cells per tile at most (45^2, 12^3)
 constexpr int kCellWarps = 4;      // warps per block of k_cells
 
 template <int D>
 __host__ __device__ constexpr int cell_dim_max() {
-  return D == 2 ? 16 : 6;
+  return D == 2 ? 45 : 12;
 }
 
 template <int D>
@@ -606,15 +746,36 @@ __device__ __forceinline__ void load_geom(const SweepArgs& a, int t, float* lo, 
   }
 }
 
-// One warp per tile: cell of every point, cell ranges and member boxes, and
-// the layout positions (a counting sort by cell inside the tile's range).
+// Exclusive scan of cnt[0..S) in place by one warp (any S).
+__device__ void warp_scan_range(int* cnt, int S) {
+  const int lane = threadIdx.x & 31;
+  const int per = (S + 31) / 32;
+  const int lo = min(lane * per, S), hi = min(lo + per, S);
+  int sum = 0;
+  for (int k = lo; k < hi; ++k)
+    sum += cnt[k];
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o)
+      incl += y;
+  }
+  int run = incl - sum;
+  for (int k = lo; k < hi; ++k) {
+    const int v = cnt[k];
+    cnt[k] = run;
+    run += v;
+  }
+}
+
+// One warp per tile: cell of every point, the layout positions (a counting
+// sort by cell inside the tile's range), cell ranges and member boxes.
 template <int D>
 __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a) {
   __shared__ int s_cnt[kCellWarps][kCellSlots];
-  __shared__ int s_box[kCellWarps][kCellSlots * 2 * D];  // ordered ints: min planes, then max
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* cnt = s_cnt[warp];
-  int* box = s_box[warp];
   const int64_t n = a.n;
   const int64_t stride = (int64_t)gridDim.x * kCellWarps;
   for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
@@ -644,59 +805,28 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
         a.cell_geom[2 * t + 1] = make_float4(inv[1], inv[D - 1], 0.0f, 0.0f);
       }
     }
-    for (int c = lane; c < kCellSlots; c += 32) {
+    const int S = D == 2 ? s * s : s * s * s;
+    for (int c = lane; c < S; c += 32)
       cnt[c] = 0;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        box[d * kCellSlots + c] = INT_MAX;
-        box[(D + d) * kCellSlots + c] = INT_MIN;
-      }
-    }
     __syncwarp();
     for (int i = lane; i < m; i += 32) {
       const int q = begin + i;
       int c = 0;
-      bool finite_box = true;
-      float x[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) {
-        x[d] = a.sx[d * n + q];
-        c = c * s + cell_coord(x[d], lo[d], inv[d], s);
-        finite_box &= x[d] == x[d];
-      }
+      for (int d = 0; d < D; ++d)
+        c = c * s + cell_coord(a.sx[d * n + q], lo[d], inv[d], s);
       atomicAdd(&cnt[c], 1);
-      if (finite_box) {  // a point with a NaN coordinate is never within reach
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          atomicMin(&box[d * kCellSlots + c], f2ord(x[d]));
-          atomicMax(&box[(D + d) * kCellSlots + c], f2ord(x[d]));
-        }
-      }
       a.cell_slot[q] = begin + c;
     }
     __syncwarp();
-    warp_scan_counts<kCellSlots>(cnt);
+    warp_scan_range(cnt, S);
     __syncwarp();
-    const int S = D == 2 ? s * s : s * s * s;
     for (int c = lane; c < S; c += 32) {
       CellInfo ci;
       ci.start = begin + cnt[c];
-      ci.end = begin + (c + 1 < kCellSlots ? cnt[c + 1] : m);
+      ci.end = begin + (c + 1 < S ? cnt[c + 1] : m);
       ci.maxkey = 0ull;
       a.cell_info[begin + c] = ci;
-      float mn[D], mx[D];
-      const bool empty = box[c] == INT_MAX;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        mn[d] = empty ? INFINITY : ord2f(box[d * kCellSlots + c]);
-        mx[d] = empty ? -INFINITY : ord2f(box[(D + d) * kCellSlots + c]);
-      }
-      if (D == 2) {
-        a.cell_box[begin + c] = make_float4(mn[0], mn[1], mx[0], mx[1]);
-      } else {
-        a.cell_box[2 * (begin + c)] = make_float4(mn[0], mn[1], mn[D - 1], mx[0]);
-        a.cell_box[2 * (begin + c) + 1] = make_float4(mx[1], mx[D - 1], 0.0f, 0.0f);
-      }
     }
     __syncwarp();
     for (int i = lane; i < m; i += 32) {
@@ -704,6 +834,42 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
       const int pos = begin + atomicAdd(&cnt[a.cell_slot[q] - begin], 1);
       a.nh_pos[q] = pos;
       a.nh_q[pos] = q;
+    }
+    __syncwarp();
+    // Member boxes. A point with a NaN coordinate is never within reach and
+    // is left out; a cell without other members gets an empty box (+inf, -inf).
+    for (int c = lane; c < S; c += 32) {
+      const int c_end = c + 1 < S ? cnt[c] : m;  // cursors now hold the cell ends
+      const int c_begin = c > 0 ? cnt[c - 1] : 0;
+      float mn[D], mx[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        mn[d] = INFINITY;
+        mx[d] = -INFINITY;
+      }
+      for (int k = c_begin; k < c_end; ++k) {
+        const int q = a.nh_q[begin + k];
+        float x[D];
+        bool ok = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          x[d] = a.sx[d * n + q];
+          ok &= x[d] == x[d];
+        }
+        if (ok) {
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            mn[d] = fminf(mn[d], x[d]);
+            mx[d] = fmaxf(mx[d], x[d]);
+          }
+        }
+      }
+      if (D == 2) {
+        a.cell_box[begin + c] = make_float4(mn[0], mn[1], mx[0], mx[1]);
+      } else {
+        a.cell_box[2 * (begin + c)] = make_float4(mn[0], mn[1], mn[D - 1], mx[0]);
+        a.cell_box[2 * (begin + c) + 1] = make_float4(mx[1], mx[D - 1], 0.0f, 0.0f);
+      }
     }
     __syncwarp();
   }
