@@ -43,10 +43,6 @@ CONFIG = {
                 "Euclidean; one tile grid per event",
     "l2": "inputs (~0.58 GB) exceed L2; no flush",
 }
-# Kernel launches of one run (grid init, extents, grid finalize, bin, scan,
-# scatter, tile sort, tile merge, merge copy, gather, density, nearest higher,
-# seed scan, parent init, labels).
-LAUNCHES_PER_RUN = 15
 # Algorithmic bytes per point (4-byte values), 2-D: density reads coordinates
 # and weight and writes rho (4D + 8); nearest higher reads coordinates, rho and
 # index and writes nh (4D + 12); the whole pipeline moves 20D + 64.
@@ -117,33 +113,20 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    from cluestering_b200 import replicas as R
+    r = R.from_env()
+    R.init(r, backend="nccl")
+    return r.world, r.rank, r.local
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from cluestering_b200 import replicas as R
+    R.barrier(R.from_env())
 
 
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from cluestering_b200 import replicas as R
+    return R.max_over_ranks(x, R.from_env())
 
 
 def cpu_reference(ev, sizes, budget_points: int, threads: int):
@@ -202,7 +185,8 @@ def run_ours(args, world, rank, local):
     hbm_peak, peak_kind = measured_peaks()
 
     # ---- workload, resident in HBM --------------------------------------------------------------
-    ev, sizes = W.batch_2d(n_events=args.events, seed=3 + 1000 * rank)
+    from cluestering_b200 import replicas as R
+    ev, sizes = W.batch_2d(n_events=args.events, seed=R.event_seed(rank))
     n_total = int(sizes.sum())
     coords_d = torch.from_numpy(ev.coords).to(dev)
     weights_d = torch.from_numpy(ev.weights).to(dev)
@@ -228,8 +212,10 @@ def run_ours(args, world, rank, local):
     ms = start.elapsed_time(end) / args.steps
     barrier(world)
     ms_max = max_over_ranks(ms, world)
-    value = n_total * world / (ms_max * 1e-3)
+    points_all = R.sum_over_ranks(n_total, R.from_env())
+    value = R.job_throughput(points_all, ms_max)
     n_clusters = algo.n_clusters()
+    launches_per_run = algo.kernel_launches()  # counted by the library at each launch site
 
     # ---- stage times of one profiled run (outside the timed region) -----------------------------
     algo.set_profiling(True)
@@ -255,7 +241,7 @@ def run_ours(args, world, rank, local):
         algo_h.make_clusters(h, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=hstream)
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     e2e_ms = max_over_ranks(e2e_ms, world)
-    e2e_value = n_total * world / (e2e_ms * 1e-3)
+    e2e_value = R.job_throughput(points_all, e2e_ms)
     same = bool(np.array_equal(h.cluster_index, pts.cluster_index.cpu().numpy()))
 
     extras = {}
@@ -272,12 +258,12 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(CONFIG, points_per_step=n_total * world, events_per_step=len(sizes) * world,
+        "config": dict(CONFIG, points_per_step=int(points_all), events_per_step=len(sizes) * world,
                        parallelism=f"replicas x{world} (events sharded by rank, no collective)"),
         "e2e": {"value": e2e_value, "unit": "points/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(ev.coords.nbytes + ev.weights.nbytes),
                 "d2h_bytes_per_step": int(n_total * 4), "matches_device_path": same},
-        "gpu_launches": LAUNCHES_PER_RUN * args.steps,
+        "gpu_launches": launches_per_run * args.steps,
         "n_clusters": n_clusters,
         "stage_ms": {k: round(v, 4) for k, v in stage.items()},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,

@@ -101,6 +101,7 @@ SIGNATURES = {
     "clue_workspace_bytes_for": (C.c_size_t, [C.c_int32, C.c_int64, C.c_int64, C.c_int32]),
     "clue_workspace_set_profiling": (C.c_int, [_P, C.c_int32]),
     "clue_workspace_stage_ms": (C.c_int, [_P, _P, C.c_int32]),
+    "clue_workspace_kernel_launches": (C.c_int, [_P, _P]),
     "clue_make_clusters_device": (C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P]),
     "clue_make_clusters_host": (C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P]),
     "clue_make_clusters_batched_device": (

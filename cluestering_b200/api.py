@@ -424,6 +424,12 @@ class Clusterer:
         L.check(L.load().clue_workspace_bytes(self._workspace(), C.byref(b)))
         return b.value
 
+    def kernel_launches(self) -> int:
+        """CUDA kernels the last make_clusters enqueued."""
+        k = C.c_int64()
+        L.check(L.load().clue_workspace_kernel_launches(self._workspace(), C.byref(k)))
+        return k.value
+
 
 # ---------------------------------------------------------------------------
 # Serving (continuous batching; no counterpart in the reference)

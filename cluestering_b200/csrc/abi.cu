@@ -485,8 +485,10 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   io.rho = pts->rho;
   io.nh = pts->nearest_higher;
   const RunParams prm = make_run_params(params, pts);
+  reset_launch_count();
   if ((e = launch_run(sh, prm, io, ws->b, st, ws->profiling ? ws->marks : nullptr)) != cudaSuccess)
     return fail_cuda(e, "kernel launch");
+  ws->last_launches = launch_count();
   // Seed count and status word come back with the run (read when needed).
   cudaMemcpyAsync(&ws->info->n_seeds, ws->b.counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
                   st);
@@ -708,6 +710,13 @@ clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t
     if (e != cudaSuccess)
       return fail_cuda(e, "cudaEventElapsedTime");
   }
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_kernel_launches(const clue_workspace* ws, int64_t* launches) {
+  if (!ws || !launches)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  *launches = ws->has_run ? ws->last_launches : 0;
   return CLUE_OK;
 }
 

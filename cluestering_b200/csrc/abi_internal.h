@@ -31,6 +31,7 @@ struct clue_workspace {
   int64_t last_n = 0;
   std::vector<clue_impl::EventDesc> last_events;
   const int32_t* last_labels = nullptr;  // device cluster ids of the last run
+  int64_t last_launches = 0;             // kernels the last run enqueued
 };
 
 namespace clue_impl {

@@ -143,4 +143,10 @@ cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t
 
 int scan_blocks_for(int64_t n);
 
+// Kernel launches enqueued by the calling thread since its last reset: every
+// launch site counts itself, and a run resets the count before it starts.
+void reset_launch_count();
+int64_t launch_count();
+void count_launches(int k);
+
 }  // namespace clue_impl

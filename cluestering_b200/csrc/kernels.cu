@@ -588,6 +588,19 @@ __global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int
 // Seeds and labels: core/detail/ClusteringKernels.hpp:293-343, :419-446
 // ---------------------------------------------------------------------------
 
+// One round of pointer jumping over the whole follower tree: every point moves
+// its parent to its grandparent. Every write stores an ancestor, so rounds may
+// overlap reads of updated entries; each round at least halves every path.
+__global__ void k_jump(int64_t n, int32_t* parent) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const int p = parent[s];
+    const int pp = __ldcg(&parent[p]);
+    if (pp != p)
+      parent[s] = pp;
+  }
+}
+
 // Root of each point's nearest-higher chain by pointer jumping with path
 // halving: every write stores an ancestor, so concurrent updates stay valid
 // and every step moves strictly up the tree. The tree is walked in the
@@ -658,6 +671,7 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
   if (n == 0)
     return cudaMemsetAsync(total, 0, sizeof(int32_t), st);
   k_scan<<<blocks, kThreads, 0, st>>>(in, out, n, b.scan_desc, b.counters, total, b.status);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -679,12 +693,19 @@ cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* i
   k_tile_merge<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, ids, b.merge_tmp);
   k_tile_merge_copy<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, b.merge_tmp,
                                               ids);
+  count_launches(4);
   return cudaGetLastError();
 }
+
+thread_local int64_t t_launches = 0;
 
 }  // namespace
 
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
+
+void reset_launch_count() { t_launches = 0; }
+int64_t launch_count() { return t_launches; }
+void count_launches(int k) { t_launches += k; }
 
 // utils/detail/get_clusters.hpp:24-49 on the device: cluster -> points as CSR,
 // point ids ascending within a cluster (the order the reference's serial
@@ -701,6 +722,7 @@ cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t
   if ((e = cudaMemsetAsync(count, 0, sizeof(int32_t) * n_clusters, st)))
     return e;
   k_hist<<<grid_for(n), kThreads, 0, st>>>(labels, n, count);
+  count_launches(1);
   if ((e = cudaGetLastError()))
     return e;
   if ((e = scan(count, offsets, n_clusters, offsets + n_clusters, b, st)))
@@ -708,6 +730,7 @@ cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t
   if ((e = cudaMemcpyAsync(cursor, offsets, sizeof(int32_t) * n_clusters, cudaMemcpyDeviceToDevice, st)))
     return e;
   k_scatter<<<grid_for(n), kThreads, 0, st>>>(labels, n, cursor, points);
+  count_launches(1);
   if ((e = cudaGetLastError()))
     return e;
   return sort_segments(offsets, n_clusters, points, b, st);
@@ -720,6 +743,7 @@ cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
     return cudaSuccess;
   k_localize<<<grid_for(n), kThreads, 0, st>>>(b.events, b.point_event, b.seed_rank, n,
                                               cluster_index, nh);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -738,7 +762,11 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     if (e_ != cudaSuccess)        \
       return e_;                  \
   } while (0)
-#define CLUE_LAUNCHED() CLUE_CHECK(cudaGetLastError())
+#define CLUE_LAUNCHED()                 \
+  do {                                  \
+    count_launches(1);                  \
+    CLUE_CHECK(cudaGetLastError());     \
+  } while (0)
 #define CLUE_MARK(i)                             \
   do {                                           \
     if (marks)                                   \
@@ -818,6 +846,13 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // seeds and labels
   CLUE_CHECK(scan(b.seed_flag, b.seed_rank, n, b.counters + 1, b, st));
+  // Large runs first shorten every chain with whole-array jumping rounds, so
+  // the per-point walks below take a few steps; small runs walk directly.
+  const int jump_rounds = n >= (int64_t)1 << 22 ? 3 : n >= (int64_t)1 << 18 ? 2 : 0;
+  for (int r = 0; r < jump_rounds; ++r) {
+    k_jump<<<grid_for(n), kThreads, 0, st>>>(n, b.parent);
+    CLUE_LAUNCHED();
+  }
   k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.perm, b.seed_flag, b.seed_rank,
                                              b.point_event, io.cluster_index, b.seeds,
                                              b.seed_event, b.status);

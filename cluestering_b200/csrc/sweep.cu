@@ -17,6 +17,7 @@
 // candidate load is one broadcast and the loops do not diverge.
 #include <cfloat>
 
+#include "engine.h"
 #include "sweep.cuh"
 
 namespace clue_impl {
@@ -170,27 +171,33 @@ __global__ void __launch_bounds__(kThreads) k_work_order(const RunParams p, cons
         local -= own[d] * g.stride[d];
       }
     }
+    // the cell search of the nearest higher visits points in layout order and
+    // needs no work order of its own
+    const bool nh_order = a.nh_pos == nullptr;
     for (int s = begin + threadIdx.x; s < end; s += blockDim.x) {
       float xi[D], si[D];
       load_point<D>(p, a, s, xi, si);
       int inf[D], sup[D];
       search_box<D>(g, p, xi, si, p.dc, inf, sup);
       const int cd = box_class<D>(g, own, inf, sup);
-      search_box<D>(g, p, xi, si, p.dm, inf, sup);
-      const int cn = box_class<D>(g, own, inf, sup);
       a.cls_dens[s] = cd;
-      a.cls_nh[s] = cn;
       atomicAdd(&cnt[0][cd], 1);
-      atomicAdd(&cnt[1][cn], 1);
+      if (nh_order) {
+        search_box<D>(g, p, xi, si, p.dm, inf, sup);
+        const int cn = box_class<D>(g, own, inf, sup);
+        a.cls_nh[s] = cn;
+        atomicAdd(&cnt[1][cn], 1);
+      }
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5;
-    if (warp < 2)
+    if (warp < (nh_order ? 2 : 1))
       warp_scan_counts<E>(cnt[warp]);
     __syncthreads();
     for (int s = begin + threadIdx.x; s < end; s += blockDim.x) {
       a.work_dens[begin + atomicAdd(&cnt[0][a.cls_dens[s]], 1)] = s;
-      a.work_nh[begin + atomicAdd(&cnt[1][a.cls_nh[s]], 1)] = s;
+      if (nh_order)
+        a.work_nh[begin + atomicAdd(&cnt[1][a.cls_nh[s]], 1)] = s;
     }
     __syncthreads();
   }
@@ -429,20 +436,65 @@ __device__ __forceinline__ void density_add(const RunParams& p, const float* xi,
   }
 }
 
-constexpr int kRing = 4;       // chunks of 32 candidate records in flight per warp
+// (a, b) as one 64-bit register pair, the operand of the f32x2 instructions.
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+
+// Streamed form of density_add: xi_xy holds (x_i, y_i) packed, the record
+// arrives as two packed halves {(x, y), (z or v, v or w)}; the arithmetic is
+// that of sq_dist and density_add.
+template <int D, int KIND>
+__device__ __forceinline__ void density_add_packed(const RunParams& p, unsigned long long xi_xy,
+                                                   float zi, const ulonglong2& r, bool self,
+                                                   float wi, float& rho) {
+  float sx, sy;
+  asm("{\n\t.reg .b64 d, s;\n\t"
+      "sub.rn.f32x2 d, %2, %3;\n\t"
+      "mul.rn.f32x2 s, d, d;\n\t"
+      "mov.b64 {%0, %1}, s;\n\t}"
+      : "=f"(sx), "=f"(sy)
+      : "l"(xi_xy), "l"(r.x));
+  float hi_lo, hi_hi;  // the record's second half: D = 2 {v, w}; D = 3 {z, v}
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(hi_lo), "=f"(hi_hi) : "l"(r.y));
+  float d2;
+  if (D == 2) {
+    d2 = __fadd_rn(sx, sy);
+  } else {
+    const float dz = __fsub_rn(zi, hi_lo);
+    d2 = __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
+  }
+  const float v = D == 2 ? hi_lo : hi_hi;
+  if (KIND == CLUE_KERNEL_FLAT) {
+    if (d2 <= p.dc2)
+      rho = __fadd_rn(rho, self ? wi : v);
+  } else if (d2 <= p.dc2) {
+    const float k = kernel_value_in_range(p, __fsqrt_rn(d2), self);
+    rho = __fadd_rn(rho, __fmul_rn(k, v));
+  }
+}
+
+constexpr int kRing = 4;       // chunks of candidate records in flight per warp
+constexpr int kChunk = 32;     // records per chunk (kChunk / 32 per lane)
 constexpr int kMaxRows = 32;   // rows of a search box the streamed path handles
 constexpr unsigned kFullMask = 0xffffffffu;
 
-// Copies stream position c * 32 + lane (row table off/qa, row cursor rr) into
-// ring slot c % kRing, then closes the lane's commit group for chunk c.
-__device__ __forceinline__ void stream_issue(float4 (*ring)[32], const int* off, const int* qa,
+// Copies stream positions c * kChunk + lane + 32 k (row table off/qa, row
+// cursor rr) into ring slot c % kRing, then closes the lane's commit group for
+// chunk c.
+__device__ __forceinline__ void stream_issue(float4 (*ring)[kChunk], const int* off, const int* qa,
                                              const float4* rec, int c, int lane, int total,
                                              int& rr) {
-  const int pp = c * 32 + lane;
-  if (pp < total) {
-    while (pp >= off[rr + 1])
-      ++rr;
-    cp_async16(&ring[c % kRing][lane], &rec[qa[rr] + (pp - off[rr])]);
+#pragma unroll
+  for (int k = 0; k < kChunk / 32; ++k) {
+    const int pp = c * kChunk + k * 32 + lane;
+    if (pp < total) {
+      while (pp >= off[rr + 1])
+        ++rr;
+      cp_async16(&ring[c % kRing][k * 32 + lane], &rec[qa[rr] + (pp - off[rr])]);
+    }
   }
   cp_async_commit();
 }
@@ -450,19 +502,19 @@ __device__ __forceinline__ void stream_issue(float4 (*ring)[32], const int* off,
 // Local density, one point per lane. When the 32 lanes of a warp share one
 // search box (the work order groups each tile's points by box), the warp
 // streams the box's candidate records through a shared-memory ring of kRing
-// chunks of 32 records, copied asynchronously kRing - 1 chunks ahead; every
+// chunks of kChunk records, copied asynchronously kRing - 1 chunks ahead; every
 // lane reads each record from shared memory. The stream is the box's rows in
 // order, each a contiguous range of sorted positions, i.e. the reference's
 // summation order. Other warps read candidates from global memory.
 template <int D, int KIND>
-__global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, const SweepArgs a) {
-  __shared__ __align__(16) float4 s_ring[kThreads / 32][kRing][32];
+__global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p, const SweepArgs a) {
+  __shared__ __align__(16) float4 s_ring[kThreads / 32][kRing][kChunk];
   __shared__ int s_off[kThreads / 32][kMaxRows + 1];
   __shared__ int s_qa[kThreads / 32][kMaxRows];
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_dens;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float4(*ring)[32] = s_ring[warp];
+  float4(*ring)[kChunk] = s_ring[warp];
   int* off = s_off[warp];
   int* qa = s_qa[warp];
   const int64_t warps_total = (int64_t)gridDim.x * (kThreads / 32);
@@ -539,7 +591,8 @@ __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, co
           p_self = off[r] + (s - qa[r]);
         }
       }
-      const int chunks = (total + 31) >> 5;
+      const int chunks = (total + kChunk - 1) / kChunk;
+      const unsigned long long xi_xy = pack2(xi[0], xi[1]);
       int rr = 0;  // row cursor of this lane's copies
 #pragma unroll
       for (int c = 0; c < kRing - 1; ++c)
@@ -548,16 +601,16 @@ __global__ void __launch_bounds__(kThreads) k_density_fast(const RunParams p, co
         stream_issue(ring, off, qa, rec, c + kRing - 1, lane, total, rr);
         cp_async_wait<kRing - 1>();
         __syncwarp();
-        const float4* chunk = ring[c % kRing];
-        const int cnt = min(32, total - c * 32);
-        const int base = c * 32;
-        if (cnt == 32) {
+        const ulonglong2* chunk = reinterpret_cast<const ulonglong2*>(ring[c % kRing]);
+        const int cnt = min(kChunk, total - c * kChunk);
+        const int jself = p_self - c * kChunk;  // own record's place in this chunk, if any
+        if (cnt == kChunk) {
 #pragma unroll 8
-          for (int j = 0; j < 32; ++j)
-            density_add<D, KIND>(p, xi, chunk[j], base + j == p_self, wi, rho);
+          for (int j = 0; j < kChunk; ++j)
+            density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
         } else {
           for (int j = 0; j < cnt; ++j)
-            density_add<D, KIND>(p, xi, chunk[j], base + j == p_self, wi, rho);
+            density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
         }
         __syncwarp();
       }
@@ -1091,6 +1144,7 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
     return cudaSuccess;
   const int blocks = (int)std::min<int64_t>(a.n_tiles, 148 * 16);
   CLUE_DISPATCH_D(D, k_work_order, blocks, kThreads, 0, st)
+  count_launches(1);
   if (a.nh_pos) {
     const int cell_blocks =
         (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, 148 * 32));
@@ -1098,6 +1152,7 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
       k_cells<2><<<cell_blocks, kCellWarps * 32, 0, st>>>(p, a);
     else
       k_cells<3><<<cell_blocks, kCellWarps * 32, 0, st>>>(p, a);
+    count_launches(1);
   }
   return cudaGetLastError();
 }
@@ -1105,6 +1160,7 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
 template <int D>
 cudaError_t launch_density_fast(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   k_pack_density<D><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+  count_launches(2);  // this and the density kernel below
   switch (p.kernel_kind) {
     case CLUE_KERNEL_FLAT:
       k_density_fast<D, CLUE_KERNEL_FLAT><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
@@ -1125,12 +1181,14 @@ cudaError_t launch_density(int D, const RunParams& p, const SweepArgs& a, cudaSt
   if (sweep_fast_path(p))
     return D == 2 ? launch_density_fast<2>(p, a, st) : launch_density_fast<3>(p, a, st);
   CLUE_DISPATCH_D(D, k_density, grid_for(a.n), kThreads, 0, st)
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_nearest_higher(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   if (a.n == 0)
     return cudaSuccess;
+  count_launches(1);  // one kernel on every path below
   if (a.nh_pos) {
     if (D == 2)
       k_nearest_higher_cells<2><<<grid_for(a.n), kThreads, 0, st>>>(p, a);

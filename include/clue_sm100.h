@@ -150,6 +150,9 @@ size_t clue_workspace_bytes_for(int32_t ndim, int64_t n_points, int64_t n_tiles,
 #define CLUE_N_STAGES 6
 clue_status clue_workspace_set_profiling(clue_workspace* ws, int32_t enable);
 clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t capacity);
+/* Number of CUDA kernels the last run on this workspace enqueued (no reference
+ * counterpart; a check that the run executed on the GPU). */
+clue_status clue_workspace_kernel_launches(const clue_workspace* ws, int64_t* launches);
 
 /* ---- clustering ----------------------------------------------------------- */
 /* Clusterer::make_clusters(Queue&, PointsDevice&, metric, kernel)

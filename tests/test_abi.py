@@ -107,8 +107,9 @@ def test_workspace_bytes_grow_with_the_problem():
     small = lib.clue_workspace_bytes_for(2, 1000, 10, 1)
     big = lib.clue_workspace_bytes_for(2, 1000000, 8281, 1)
     assert 0 < small < big
-    # about (D + 13) 4-byte words per point plus 3 per tile
-    assert big < 1000000 * 4 * 32
+    # about 43 4-byte words per point in 2-D (sorted copies, sweep records and
+    # the nearest-higher cell layout) plus a few per tile
+    assert big < 1000000 * 4 * 48
 
 
 def test_clusters_csr_host():
