@@ -48,6 +48,10 @@ CONFIG = {
 # index and writes nh (4D + 12); the whole pipeline moves 20D + 64.
 BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4 * D + 12,
                    "pipeline": lambda D: 20 * D + 64}
+# DRAM bytes (read + write) per point of each sweep, from one ncu capture of the
+# 1,024-event batch (profiles/sweeps_batch_2d_1024ev.md: 893.8 MB and 644.2 MB
+# for 10,621,973 points); a launch's traffic grows with the points it processes.
+DRAM_BYTES_PER_POINT = {"density": 84.1, "nearest_higher": 60.6}
 
 
 def measured_peaks():
@@ -267,10 +271,12 @@ def run_ours(args, world, rank, local):
         "n_clusters": n_clusters,
         "stage_ms": {k: round(v, 4) for k, v in stage.items()},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": DRAM_BYTES_PER_POINT[dom] * n_total,
                      "peak_kind": peak_kind,
-                     "note": "sweeps are FP32-issue bound: each point tests ~10^3 candidates in "
-                             "the reference's tile order; bytes are the algorithmic minimum"},
+                     "note": "sweeps are issue/latency bound: each point tests ~855 candidates "
+                             "in the reference's tile order; achieved counts algorithmic bytes, "
+                             "traffic is ncu DRAM bytes per point scaled to this launch"},
         "clocks": clocks.summary(),
         "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": os.cpu_count() or 1,
                          "kind": "port", "sample": cpu_sample},
@@ -416,6 +422,29 @@ def run_serving(args, local):
     return out
 
 
+def run_one_tile(args):
+    """One event of 16,384 points uniform in [0, 10]^2 with a single tile (dc = 0.3): every
+    density warp streams the same 16,384 candidates, which isolates the per-candidate cost
+    (instructions per candidate = warp instructions / (512 warps x 16,384))."""
+    import torch
+
+    import cluestering_b200 as clue
+    n = 16384
+    x = np.random.default_rng(0).uniform(0, 10, (2, n)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    pts = clue.PointsDevice(torch.from_numpy(x).to(dev), torch.ones(n, device=dev))
+    algo = clue.Clusterer(0.3, 5.0, 0.3, points_per_tile=1 << 24)
+    for _ in range(max(1, args.warmup)):
+        algo.make_clusters(pts)
+    algo.set_profiling(True)
+    algo.make_clusters(pts)
+    st = algo.stage_ms()
+    print(json.dumps({"case": "one-tile", "points": n, "candidates_per_point": n,
+                      "stage_ms": {k: round(v, 4) for k, v in st.items()},
+                      "kernel_launches": algo.kernel_launches()}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,7 +462,13 @@ def main():
     ap.add_argument("--serve-linger-us", type=int, default=200)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--skip-extras", action="store_true")
+    ap.add_argument("--case", choices=["one-tile"], default=None,
+                    help="profiling case instead of the benchmark: 'one-tile' clusters one "
+                         "16,384-point event whose points all share one tile, so every warp of "
+                         "the density sweep streams the same box")
     args = ap.parse_args()
+    if args.case == "one-tile":
+        return run_one_tile(args)
     if args.impl == "reference":
         # CPU arm: rank 0 times the CPU restatement; other ranks have no work.
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")),

@@ -287,8 +287,10 @@ class Clusterer:
         self.setParameters(density_radius, min_density, outlier_distance, seeding_distance)
 
     def __del__(self):
-        if getattr(self, "_ws", None) is not None:
-            L.load().clue_workspace_destroy(self._ws)
+        ws = getattr(self, "_ws", None)
+        lib = getattr(L, "_lib", None) if L is not None else None
+        if ws is not None and lib is not None:  # at interpreter exit the module may be gone
+            lib.clue_workspace_destroy(ws)
             self._ws = None
 
     # -- parameters -----------------------------------------------------
