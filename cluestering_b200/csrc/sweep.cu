@@ -664,6 +664,51 @@ __device__ __forceinline__ void bracket(float delta, float& lo, float& hi) {
   hi = isinf(bb) ? bb : next_up(bb);
 }
 
+// Best candidate of a nearest-higher search: its squared distance d2b, key and
+// position, and a bracket (lo, hi) around d2b: every d2 <= lo has
+// sqrt_rn(d2) < sqrt_rn(d2b) and every d2 >= hi has sqrt_rn(d2) > sqrt_rn(d2b).
+struct NhBest {
+  float d2b, lo, hi;
+  int best;
+  uint64_t key_b;
+};
+
+__device__ __forceinline__ NhBest nh_none() {
+  const float inf = __int_as_float(0x7f800000);
+  return NhBest{inf, inf, inf, -1, 0ull};  // no best yet: every eligible candidate wins
+}
+
+// For d2b >= 2^-100 the bracket is d2b * (1 -+ 2^-20): with round-to-nearest
+// errors of at most 2^-24 in the product and in sqrt_rn, d2 <= fl(d2b (1 - 2^-20))
+// gives sqrt_rn(d2) <= sqrt(d2b)(1 - 6.5 * 2^-24) < sqrt_rn(d2b), and
+// symmetrically above (an overflowing hi is +inf, which only sends more
+// candidates to the exact comparison). Smaller d2b (0 for coincident points)
+// takes the exact rounding class of sqrt_rn(d2b).
+__device__ __forceinline__ void nh_take(NhBest& st, float d2, int q, uint64_t key) {
+  st.d2b = d2;
+  st.best = q;
+  st.key_b = key;
+  if (d2 >= 0x1p-100f) {
+    st.lo = __fmul_rn(d2, 0.99999904632568359375f);   // 1 - 2^-20
+    st.hi = __fmul_rn(d2, 1.00000095367431640625f);   // 1 + 2^-20
+  } else {
+    bracket(__fsqrt_rn(d2), st.lo, st.hi);
+  }
+}
+
+// ClusteringKernels.hpp:195-202 for one eligible candidate (higher key, d2 <=
+// eff2): it wins when its distance is smaller, or equal with a larger key.
+// Only squared distances inside the bracket take the exact square roots.
+__device__ __forceinline__ void nh_consider(NhBest& st, float d2, int q, uint64_t key) {
+  if (d2 <= st.lo) {
+    nh_take(st, d2, q, key);
+  } else if (d2 < st.hi) {
+    const float dist = __fsqrt_rn(d2), delta = __fsqrt_rn(st.d2b);
+    if ((dist < delta) || ((dist == delta) && (key > st.key_b)))
+      nh_take(st, d2, q, key);
+  }
+}
+
 // Nearest higher with (density, tag) as one ordered 64-bit key and distances
 // compared as squared distances. A candidate j of point i is eligible when it is
 // "higher" (key_j > key_i, which is rho_j > rho_i, or equal densities above zero
@@ -673,7 +718,7 @@ __device__ __forceinline__ void bracket(float delta, float& lo, float& hi) {
 // bracket decides all but the candidates whose squared distance falls in
 // (lo, hi); those take the exact square root.
 template <int D>
-__global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParams p,
+__global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_fast(const RunParams p,
                                                                   const SweepArgs a) {
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_nh;
@@ -699,33 +744,16 @@ __global__ void __launch_bounds__(kThreads) k_nearest_higher_fast(const RunParam
         ((nan_i || !(rho_i > 0.0f)) ? 0xffffffffu : tag_i);
     int inf[D], sup[D];
     search_box<D>(g, p, xi, zero, p.dm, inf, sup);
-    float delta = FLT_MAX;
-    float lo = __int_as_float(0x7f800000), hi = lo;  // no best yet: every eligible wins
-    int best = -1;
-    uint64_t key_b = 0;
+    NhBest bs = nh_none();
     for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
       const float4 r = __ldg(&rec[q]);
       const uint32_t tag_j = D == 2 ? __float_as_uint(r.w) : __ldg(&a.rec_tag[q]);
       const uint64_t key_j = ((uint64_t)__float_as_uint(D == 2 ? r.z : r.w) << 32) | tag_j;
       const float d2 = sq_dist<D>(xi, r);
-      const bool cand = (key_j > key_i) && (d2 <= eff2);
-      const bool clear = cand && (d2 <= lo);
-      if (cand && !clear && d2 < hi) {
-        // rounding class of delta: decide exactly
-        const float dist = __fsqrt_rn(d2);
-        if ((dist < delta) || ((dist == delta) && (best >= 0) && (key_j > key_b))) {
-          delta = dist;
-          bracket(delta, lo, hi);
-          best = q;
-          key_b = key_j;
-        }
-      } else if (clear) {
-        delta = __fsqrt_rn(d2);
-        bracket(delta, lo, hi);
-        best = q;
-        key_b = key_j;
-      }
+      if ((key_j > key_i) && (d2 <= eff2))
+        nh_consider(bs, d2, q, key_j);
     });
+    const int best = bs.best;
     const int gi = a.perm[s];
     const int nh = best >= 0 ? a.perm[best] : -1;
     a.out_nh[gi] = nh;
@@ -944,14 +972,6 @@ __device__ __forceinline__ float box_lower_bound(const float* xi, const float* m
                    __fadd_rn(__fmul_rn(gap[1], gap[1]), __fmul_rn(gap[D - 1], gap[D - 1])));
 }
 
-// Search state of one point: best candidate so far (layout position), its
-// distance and key, and the squared-distance bracket of that distance.
-struct NhBest {
-  float delta, lo, hi;
-  int best;
-  uint64_t key_b;
-};
-
 // Tests the members of one cell unless the cell is empty, holds no higher
 // key, or its box is out of reach.
 template <int D>
@@ -977,22 +997,8 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
     const uint32_t tag_j = D == 2 ? __float_as_uint(r.w) : __ldg(&a.rec_tag[q]);
     const uint64_t key_j = ((uint64_t)__float_as_uint(D == 2 ? r.z : r.w) << 32) | tag_j;
     const float d2 = sq_dist<D>(xi, r);
-    const bool cand = (key_j > key_i) && (d2 <= eff2);
-    const bool clear = cand && (d2 <= st.lo);
-    if (cand && !clear && d2 < st.hi) {
-      const float dist = __fsqrt_rn(d2);
-      if ((dist < st.delta) || ((dist == st.delta) && (st.best >= 0) && (key_j > st.key_b))) {
-        st.delta = dist;
-        bracket(dist, st.lo, st.hi);
-        st.best = q;
-        st.key_b = key_j;
-      }
-    } else if (clear) {
-      st.delta = __fsqrt_rn(d2);
-      bracket(st.delta, st.lo, st.hi);
-      st.best = q;
-      st.key_b = key_j;
-    }
+    if ((key_j > key_i) && (d2 <= eff2))
+      nh_consider(st, d2, q, key_j);
   }
 }
 
@@ -1035,7 +1041,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunP
     const int t0 = tile_id<D>(g, p, ev.tile_base, own);
 
     // no best yet: every eligible candidate wins
-    NhBest bs{FLT_MAX, __int_as_float(0x7f800000), __int_as_float(0x7f800000), -1, 0ull};
+    NhBest bs = nh_none();
 
     // Phase 0: the own cell and its neighbours in the own tile. Phase 1: every
     // tile of the search box, cells within reach only, less those of phase 0.
