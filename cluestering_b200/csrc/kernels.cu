@@ -828,7 +828,8 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.out_seed = io.is_seed;
   a.seed_flag = b.seed_flag;
   a.parent = b.parent;
-  if (sweep_cells_path(prm)) {
+  if (sweep_fast_path(prm)) {
+    a.nh_cells = sweep_cells_path(prm);
     a.nh_pos = b.nh_pos;
     a.nh_q = b.nh_q;
     a.cell_slot = b.cell_slot;

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) k_work_order(const RunParams p, cons
     }
     // the cell search of the nearest higher visits points in layout order and
     // needs no work order of its own
-    const bool nh_order = a.nh_pos == nullptr;
+    const bool nh_order = !a.nh_cells;
     for (int s = begin + threadIdx.x; s < end; s += blockDim.x) {
       float xi[D], si[D];
       load_point<D>(p, a, s, xi, si);
@@ -408,6 +408,104 @@ __device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const Gri
   }
 }
 
+// ---------------------------------------------------------------------------
+// Cell layout (fast path).
+//
+// Every tile of m points is split into s^D cells, s the largest value with
+// s^D * kCellTarget <= m (at least 1, at most cell_dim_max). A point's cell
+// comes from cell_coord, which is monotone in the coordinate; a search
+// therefore finds every point of [a, b] in the cells cell_coord(a) ..
+// cell_coord(b), whatever rounding placed it there. Each cell records the
+// bounding box of its members and (for the nearest-higher search) their
+// largest key. The density sweep uses the cells to skip candidates no lane of
+// a warp can reach; the nearest-higher search visits them nearest-first.
+// ---------------------------------------------------------------------------
+
+constexpr int kCellTarget = 2;     // average points per cell
+constexpr int kCellSlots = 2048;   // cells per tile at most (45^2, 12^3)
+constexpr int kCellWarps = 4;      // warps per block of k_cells
+
+template <int D>
+__host__ __device__ constexpr int cell_dim_max() {
+  return D == 2 ? 45 : 12;
+}
+
+template <int D>
+__device__ __forceinline__ int cells_per_dim(int m) {
+  int s = 1;
+  while (s < cell_dim_max<D>()) {
+    const int u = s + 1;
+    const int vol = D == 2 ? u * u : u * u * u;
+    if (vol * kCellTarget > m)
+      break;
+    s = u;
+  }
+  return s;
+}
+
+// Cell coordinate of x in a tile with origin lo and inverse cell width inv
+// (0 for a degenerate tile): monotone non-decreasing in x for every non-NaN x,
+// clamped to [0, s); NaN lands in cell 0.
+__device__ __forceinline__ int cell_coord(float x, float lo, float inv, int s) {
+  float u = __fmul_rn(__fsub_rn(x, lo), inv);
+  u = fminf(fmaxf(u, 0.0f), (float)(s - 1));
+  return (int)u;
+}
+
+// Origin and inverse cell width of the tiles' cells, dimension d.
+__device__ __forceinline__ void cell_axis(const GridDesc& g, int b, int s, int d, float& lo,
+                                          float& inv) {
+  lo = __fadd_rn(g.minv[d], __fmul_rn((float)b, g.tile[d]));
+  const float v = __fdiv_rn((float)s, g.tile[d]);
+  inv = (g.tile[d] > 0.0f && v < INFINITY) ? v : 0.0f;
+}
+
+template <int D>
+__device__ __forceinline__ void load_geom(const SweepArgs& a, int t, float* lo, float* inv) {
+  const float4 g0 = a.cell_geom[D == 2 ? t : 2 * t];
+  if (D == 2) {
+    lo[0] = g0.x, lo[1] = g0.y, inv[0] = g0.z, inv[1] = g0.w;
+  } else {
+    const float4 g1 = a.cell_geom[2 * t + 1];
+    lo[0] = g0.x, lo[1] = g0.y, lo[D - 1] = g0.z, inv[0] = g0.w, inv[1] = g1.x, inv[D - 1] = g1.y;
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void load_box(const SweepArgs& a, int slot, float* mn, float* mx) {
+  const float4 b0 = a.cell_box[D == 2 ? slot : 2 * slot];
+  if (D == 2) {
+    mn[0] = b0.x, mn[1] = b0.y, mx[0] = b0.z, mx[1] = b0.w;
+  } else {
+    const float4 b1 = a.cell_box[2 * slot + 1];
+    mn[0] = b0.x, mn[1] = b0.y, mn[D - 1] = b0.z, mx[0] = b0.w, mx[1] = b1.x, mx[D - 1] = b1.y;
+  }
+}
+
+// Lower bound of the squared distance from xi to any member of a cell, with
+// the operations of sq_dist: per dimension the gap to the box is at most
+// |fl(x_i - x_j)| of every member (rounding is monotone), and squares and the
+// right fold are monotone too.
+template <int D>
+__device__ __forceinline__ float box_lower_bound(const float* xi, const float* mn, const float* mx) {
+  float gap[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    gap[d] = fmaxf(fmaxf(__fsub_rn(mn[d], xi[d]), __fsub_rn(xi[d], mx[d])), 0.0f);
+  if (D == 2)
+    return __fadd_rn(__fmul_rn(gap[0], gap[0]), __fmul_rn(gap[1], gap[1]));
+  return __fadd_rn(__fmul_rn(gap[0], gap[0]),
+                   __fadd_rn(__fmul_rn(gap[1], gap[1]), __fmul_rn(gap[D - 1], gap[D - 1])));
+}
+
+// |x_j - x_i| <= reach(bound2) in every coordinate for every point with
+// fl(d2) <= bound2: each square and sum is rounded to nearest, so
+// |x_j - x_i| <= sqrt(bound2) (1 + 2^-22); the factor 1 + 10^-6 and the
+// absolute 10^-19 (square roots near the smallest normal) cover that, rounded up.
+__device__ __forceinline__ float reach(float bound2) {
+  return __fadd_ru(__fmul_ru(__fsqrt_ru(bound2), 1.000001f), 1e-19f);
+}
+
 // Asynchronous 16-byte global -> shared copies (per thread, completion by
 // commit groups).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -631,7 +729,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
     const uint32_t kbits = rho_key(rho);
     const float key = __uint_as_float(kbits);
     int pos = s;
-    if (a.nh_pos) {
+    if (a.nh_cells) {
       pos = a.nh_pos[s];
       atomicMax(&a.cell_info[a.cell_slot[s]].maxkey, ((unsigned long long)kbits << 32) | tag);
     }
@@ -765,67 +863,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_fast(const RunPa
   }
 }
 
-// ---------------------------------------------------------------------------
-// Cell layout of the nearest-higher search (fast path without user tags).
-//
-// Every tile of m points is split into s^D cells, s the largest value with
-// s^D * kCellTarget <= m (at least 1, at most cell_dim_max). A point's cell
-// comes from cell_coord, which is monotone in the coordinate; the search
-// therefore finds every point of [a, b] in the cells cell_coord(a) ..
-// cell_coord(b), whatever rounding placed it there. Each cell records the
-// bounding box of its members and their largest key, and a cell is skipped
-// when its box is provably out of reach or none of its keys is higher.
-// ---------------------------------------------------------------------------
-
-constexpr int kCellTarget = 2;     // average points per cell
-constexpr int kCellSlots = 2048;   // cells per tile at most (45^2, 12^3)
-constexpr int kCellWarps = 4;      // warps per block of k_cells
-
-template <int D>
-__host__ __device__ constexpr int cell_dim_max() {
-  return D == 2 ? 45 : 12;
-}
-
-template <int D>
-__device__ __forceinline__ int cells_per_dim(int m) {
-  int s = 1;
-  while (s < cell_dim_max<D>()) {
-    const int u = s + 1;
-    const int vol = D == 2 ? u * u : u * u * u;
-    if (vol * kCellTarget > m)
-      break;
-    s = u;
-  }
-  return s;
-}
-
-// Cell coordinate of x in a tile with origin lo and inverse cell width inv
-// (0 for a degenerate tile): monotone non-decreasing in x for every non-NaN x,
-// clamped to [0, s); NaN lands in cell 0.
-__device__ __forceinline__ int cell_coord(float x, float lo, float inv, int s) {
-  float u = __fmul_rn(__fsub_rn(x, lo), inv);
-  u = fminf(fmaxf(u, 0.0f), (float)(s - 1));
-  return (int)u;
-}
-
-// Origin and inverse cell width of the tiles' cells, dimension d.
-__device__ __forceinline__ void cell_axis(const GridDesc& g, int b, int s, int d, float& lo,
-                                          float& inv) {
-  lo = __fadd_rn(g.minv[d], __fmul_rn((float)b, g.tile[d]));
-  const float v = __fdiv_rn((float)s, g.tile[d]);
-  inv = (g.tile[d] > 0.0f && v < INFINITY) ? v : 0.0f;
-}
-
-template <int D>
-__device__ __forceinline__ void load_geom(const SweepArgs& a, int t, float* lo, float* inv) {
-  const float4 g0 = a.cell_geom[D == 2 ? t : 2 * t];
-  if (D == 2) {
-    lo[0] = g0.x, lo[1] = g0.y, inv[0] = g0.z, inv[1] = g0.w;
-  } else {
-    const float4 g1 = a.cell_geom[2 * t + 1];
-    lo[0] = g0.x, lo[1] = g0.y, lo[D - 1] = g0.z, inv[0] = g0.w, inv[1] = g1.x, inv[D - 1] = g1.y;
-  }
-}
 
 // Exclusive scan of cnt[0..S) in place by one warp (any S).
 __device__ void warp_scan_range(int* cnt, int S) {
@@ -850,13 +887,23 @@ __device__ void warp_scan_range(int* cnt, int S) {
   }
 }
 
+__device__ __forceinline__ unsigned lane_mask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
 // One warp per tile: cell of every point, the layout positions (a counting
-// sort by cell inside the tile's range), cell ranges and member boxes.
+// sort by cell inside the tile's range), cell ranges and member boxes, and the
+// density sweep's work order for the tile.
 template <int D>
 __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a) {
+  constexpr int E = box_classes<D>();
   __shared__ int s_cnt[kCellWarps][kCellSlots];
+  __shared__ int s_cls[kCellWarps][E];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* cnt = s_cnt[warp];
+  int* ccnt = s_cls[warp];
   const int64_t n = a.n;
   const int64_t stride = (int64_t)gridDim.x * kCellWarps;
   for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
@@ -868,13 +915,14 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
     const GridDesc& g = a.grids[ev.grid];
     const int s = cells_per_dim<D>(m);
     float lo[D], inv[D];
+    int own[D];
     {
       int local = (int)t - ev.tile_base;
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        const int b = local / g.stride[d];
-        local -= b * g.stride[d];
-        cell_axis(g, b, s, d, lo[d], inv[d]);
+        own[d] = local / g.stride[d];
+        local -= own[d] * g.stride[d];
+        cell_axis(g, own[d], s, d, lo[d], inv[d]);
       }
     }
     if (lane == 0) {
@@ -953,23 +1001,47 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
       }
     }
     __syncwarp();
-  }
-}
-
-// Lower bound of the squared distance from xi to any member of a cell, with
-// the operations of sq_dist: per dimension the gap to the box is at most
-// |fl(x_i - x_j)| of every member (rounding is monotone), and squares and the
-// right fold are monotone too.
-template <int D>
-__device__ __forceinline__ float box_lower_bound(const float* xi, const float* mn, const float* mx) {
-  float gap[D];
+    // Density work order: the tile's points grouped by search-box class (the
+    // lanes of a warp share one box) and in cell-layout order inside a class
+    // (they are neighbours, so the cells within reach of the warp are few). A
+    // stable counting sort: rounds of 32 layout positions, in order, ranked
+    // within a round by __match_any_sync.
+    for (int c = lane; c < E; c += 32)
+      ccnt[c] = 0;
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) {
+      const int q = a.nh_q[begin + i];
+      float xq[D];
+      const float zero[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-  for (int d = 0; d < D; ++d)
-    gap[d] = fmaxf(fmaxf(__fsub_rn(mn[d], xi[d]), __fsub_rn(xi[d], mx[d])), 0.0f);
-  if (D == 2)
-    return __fadd_rn(__fmul_rn(gap[0], gap[0]), __fmul_rn(gap[1], gap[1]));
-  return __fadd_rn(__fmul_rn(gap[0], gap[0]),
-                   __fadd_rn(__fmul_rn(gap[1], gap[1]), __fmul_rn(gap[D - 1], gap[D - 1])));
+      for (int d = 0; d < D; ++d)
+        xq[d] = a.sx[d * n + q];
+      int inf[D], sup[D];
+      search_box<D>(g, p, xq, zero, p.dc, inf, sup);
+      const int c = box_class<D>(g, own, inf, sup);
+      a.cls_dens[begin + i] = c;
+      atomicAdd(&ccnt[c], 1);
+    }
+    __syncwarp();
+    warp_scan_range(ccnt, E);
+    __syncwarp();
+    for (int base = 0; base < m; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < m;
+      const int c = valid ? a.cls_dens[begin + i] : -1;
+      const unsigned grp = __match_any_sync(kFullMask, c);
+      const int leader = __ffs(grp) - 1;
+      int first = 0;
+      if (valid && lane == leader) {
+        first = ccnt[c];
+        ccnt[c] = first + __popc(grp);
+      }
+      first = __shfl_sync(kFullMask, first, leader);
+      if (valid)
+        a.work_dens[begin + first + __popc(grp & lane_mask_lt())] = a.nh_q[begin + i];
+      __syncwarp();
+    }
+  }
 }
 
 // Tests the members of one cell unless the cell is empty, holds no higher
@@ -981,13 +1053,7 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
   if (ci.start == ci.end || ci.maxkey <= key_i)
     return;
   float mn[D], mx[D];
-  const float4 b0 = a.cell_box[D == 2 ? slot : 2 * slot];
-  if (D == 2) {
-    mn[0] = b0.x, mn[1] = b0.y, mx[0] = b0.z, mx[1] = b0.w;
-  } else {
-    const float4 b1 = a.cell_box[2 * slot + 1];
-    mn[0] = b0.x, mn[1] = b0.y, mn[D - 1] = b0.z, mx[0] = b0.w, mx[1] = b1.x, mx[D - 1] = b1.y;
-  }
+  load_box<D>(a, slot, mn, mx);
   const float lb2 = box_lower_bound<D>(xi, mn, mx);
   if (lb2 > eff2 || lb2 >= st.hi)
     return;
@@ -1064,8 +1130,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunP
         float glo[D], ginv[D];
         load_geom<D>(a, t, glo, ginv);
         // |x_j - x_i| <= R for every member that can still win (d2 <= bound2)
-        const float bound2 = fminf(eff2, bs.hi);
-        const float R = __fadd_ru(__fmul_ru(__fsqrt_ru(bound2), 1.000001f), 1e-19f);
+        const float R = reach(fminf(eff2, bs.hi));
         int c_lo[D], c_hi[D], c[D];
 #pragma unroll
         for (int d = 0; d < D; ++d) {
@@ -1148,9 +1213,13 @@ bool sweep_cells_path(const RunParams& p) { return sweep_fast_path(p) && !p.has_
 cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   if (a.n == 0)
     return cudaSuccess;
-  const int blocks = (int)std::min<int64_t>(a.n_tiles, 148 * 16);
-  CLUE_DISPATCH_D(D, k_work_order, blocks, kThreads, 0, st)
-  count_launches(1);
+  // With cells, k_cells writes the density work order; k_work_order is still
+  // needed for the nearest-higher order when the cell search is off (tags).
+  if (!a.nh_cells) {
+    const int blocks = (int)std::min<int64_t>(a.n_tiles, 148 * 16);
+    CLUE_DISPATCH_D(D, k_work_order, blocks, kThreads, 0, st)
+    count_launches(1);
+  }
   if (a.nh_pos) {
     const int cell_blocks =
         (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, 148 * 32));
@@ -1195,7 +1264,7 @@ cudaError_t launch_nearest_higher(int D, const RunParams& p, const SweepArgs& a,
   if (a.n == 0)
     return cudaSuccess;
   count_launches(1);  // one kernel on every path below
-  if (a.nh_pos) {
+  if (a.nh_cells) {
     if (D == 2)
       k_nearest_higher_cells<2><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
     else

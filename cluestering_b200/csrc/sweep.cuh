@@ -45,6 +45,10 @@ struct SweepArgs {
   // reordered cell by cell inside the tile's range. A tile starting at sorted
   // position b keeps its cells in slots b .. b + s^D - 1 (s^D never exceeds
   // the tile's point count).
+  // The cells are built for every fast-path run (the density sweep uses them to
+  // skip out-of-reach candidates); the nearest-higher search runs over them
+  // when nh_cells is set (no user tags), and then its records are in cell order.
+  bool nh_cells;
   int32_t* nh_pos;        // sorted position -> layout position
   int32_t* nh_q;          // layout position -> sorted position
   int32_t* cell_slot;     // sorted position -> slot of its cell
