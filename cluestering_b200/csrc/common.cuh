@@ -17,6 +17,10 @@
 namespace clue_impl {
 
 constexpr int kMaxDim = CLUE_MAX_DIM;
+// Tiles of more points than this are "large": the tile sort lists them
+// (DeviceBuffers::large_tiles) and the kernels that work tile by tile give
+// each of them a whole block instead of one warp.
+constexpr int kLargeTilePoints = 256;
 
 // ---------------------------------------------------------------------------
 // Tables the host builds for a run

@@ -390,7 +390,7 @@ __device__ __forceinline__ void warp_rank_sort(int32_t* seg, int m, int* ids, in
 // kWarpSortCap ids are rank-sorted by the warp with no block barrier; larger
 // tiles are listed for k_tile_sort_large. Tiles already in order (one warp of
 // the scatter placed all of them) are left as they are.
-constexpr int kWarpSortCap = 256;
+constexpr int kWarpSortCap = kLargeTilePoints;
 __global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offset, int64_t n_tiles,
                                                         int32_t* perm, int32_t* large,
                                                         int32_t* large_count) {
@@ -809,6 +809,9 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.work_nh = b.work_nh;
   a.cls_dens = b.cls_dens;
   a.cls_nh = b.cls_nh;
+  a.queue = b.counters + 4;
+  a.large_tiles = b.large_tiles;  // listed by sort_segments above
+  a.large_count = b.counters + 3;
   a.rec_dens = b.rec_dens;
   a.rec_nh = b.rec_nh;
   a.rec_tag = b.rec_tag;

@@ -364,6 +364,8 @@ __device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
 
 template <int D>
 __global__ void __launch_bounds__(kThreads) k_pack_density(const RunParams p, const SweepArgs a) {
+  if (blockIdx.x == 0 && threadIdx.x < 2)
+    a.queue[threadIdx.x] = 0;  // the sweeps that follow start with no item taken
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
        s += (int64_t)gridDim.x * blockDim.x) {
     const float w = a.sw[s];
@@ -541,13 +543,12 @@ __device__ __forceinline__ unsigned long long pack2(float a, float b) {
   return r;
 }
 
-// Streamed form of density_add: xi_xy holds (x_i, y_i) packed, the record
-// arrives as two packed halves {(x, y), (z or v, v or w)}; the arithmetic is
-// that of sq_dist and density_add.
-template <int D, int KIND>
-__device__ __forceinline__ void density_add_packed(const RunParams& p, unsigned long long xi_xy,
-                                                   float zi, const ulonglong2& r, bool self,
-                                                   float wi, float& rho) {
+// Squared distance and contribution weight of a streamed record: xi_xy holds
+// (x_i, y_i) packed, the record arrives as two packed halves {(x, y), (z or v,
+// v or w)}; the arithmetic is that of sq_dist.
+template <int D>
+__device__ __forceinline__ float packed_d2(unsigned long long xi_xy, float zi, const ulonglong2& r,
+                                           float& v) {
   float sx, sy;
   asm("{\n\t.reg .b64 d, s;\n\t"
       "sub.rn.f32x2 d, %2, %3;\n\t"
@@ -557,14 +558,20 @@ __device__ __forceinline__ void density_add_packed(const RunParams& p, unsigned 
       : "l"(xi_xy), "l"(r.x));
   float hi_lo, hi_hi;  // the record's second half: D = 2 {v, w}; D = 3 {z, v}
   asm("mov.b64 {%0, %1}, %2;" : "=f"(hi_lo), "=f"(hi_hi) : "l"(r.y));
-  float d2;
-  if (D == 2) {
-    d2 = __fadd_rn(sx, sy);
-  } else {
-    const float dz = __fsub_rn(zi, hi_lo);
-    d2 = __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
-  }
-  const float v = D == 2 ? hi_lo : hi_hi;
+  v = D == 2 ? hi_lo : hi_hi;
+  if (D == 2)
+    return __fadd_rn(sx, sy);
+  const float dz = __fsub_rn(zi, hi_lo);
+  return __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
+}
+
+// Streamed form of density_add (same arithmetic).
+template <int D, int KIND>
+__device__ __forceinline__ void density_add_packed(const RunParams& p, unsigned long long xi_xy,
+                                                   float zi, const ulonglong2& r, bool self,
+                                                   float wi, float& rho) {
+  float v;
+  const float d2 = packed_d2<D>(xi_xy, zi, r, v);
   if (KIND == CLUE_KERNEL_FLAT) {
     if (d2 <= p.dc2)
       rho = __fadd_rn(rho, self ? wi : v);
@@ -597,6 +604,42 @@ __device__ __forceinline__ void stream_issue(float4 (*ring)[kChunk], const int* 
   cp_async_commit();
 }
 
+// One streamed chunk for the kernels with an exponential (Gaussian,
+// exponential). The lanes of a warp seldom have the same candidates in range,
+// so evaluating the kernel inside the candidate loop would run it whenever any
+// lane is in range. Each lane first marks its in-range records of the chunk,
+// then evaluates the kernel on its own marked records only, lowest first: the
+// same additions in the same order as density_add_packed.
+template <int D, int KIND>
+__device__ __forceinline__ void density_chunk_masked(const RunParams& p, unsigned long long xi_xy,
+                                                     float zi, const ulonglong2* chunk, int cnt,
+                                                     int jself, float& rho) {
+  static_assert(kChunk == 32, "one mask bit per record of a chunk");
+  unsigned m = 0;
+  if (cnt == kChunk) {
+#pragma unroll 8
+    for (int j = 0; j < kChunk; ++j) {
+      float v;
+      if (packed_d2<D>(xi_xy, zi, chunk[j], v) <= p.dc2)
+        m |= 1u << j;
+    }
+  } else {
+    for (int j = 0; j < cnt; ++j) {
+      float v;
+      if (packed_d2<D>(xi_xy, zi, chunk[j], v) <= p.dc2)
+        m |= 1u << j;
+    }
+  }
+  while (m) {
+    const int j = __ffs(m) - 1;
+    m &= m - 1;
+    float v;
+    const float d2 = packed_d2<D>(xi_xy, zi, chunk[j], v);
+    const float k = kernel_value_in_range(p, __fsqrt_rn(d2), j == jself);
+    rho = __fadd_rn(rho, __fmul_rn(k, v));
+  }
+}
+
 // Local density, one point per lane. When the 32 lanes of a warp share one
 // search box (the work order groups each tile's points by box), the warp
 // streams the box's candidate records through a shared-memory ring of kRing
@@ -615,9 +658,16 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
   float4(*ring)[kChunk] = s_ring[warp];
   int* off = s_off[warp];
   int* qa = s_qa[warp];
-  const int64_t warps_total = (int64_t)gridDim.x * (kThreads / 32);
-  for (int64_t w0 = ((int64_t)blockIdx.x * (kThreads / 32) + warp) * 32; w0 < n; w0 += warps_total * 32) {
-    const int64_t w = w0 + lane;
+  const int64_t n_items = (n + 31) / 32;
+  for (;;) {
+    // next item of 32 work positions: warps of light boxes take more items
+    int64_t item = 0;
+    if (lane == 0)
+      item = atomicAdd(reinterpret_cast<unsigned*>(&a.queue[0]), 1u);
+    item = __shfl_sync(kFullMask, item, 0);
+    if (item >= n_items)
+      break;
+    const int64_t w = item * 32 + lane;
     const bool active = w < n;
     int s = active ? a.work_dens[w] : 0;
     // idle lanes shadow lane 0 (the shuffle runs on every lane: a full-mask
@@ -702,7 +752,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
         const ulonglong2* chunk = reinterpret_cast<const ulonglong2*>(ring[c % kRing]);
         const int cnt = min(kChunk, total - c * kChunk);
         const int jself = p_self - c * kChunk;  // own record's place in this chunk, if any
-        if (cnt == kChunk) {
+        if (KIND != CLUE_KERNEL_FLAT) {
+          density_chunk_masked<D, KIND>(p, xi_xy, xi[2], chunk, cnt, jself, rho);
+        } else if (cnt == kChunk) {
 #pragma unroll 8
           for (int j = 0; j < kChunk; ++j)
             density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
@@ -893,154 +945,185 @@ __device__ __forceinline__ unsigned lane_mask_lt() {
   return m;
 }
 
-// One warp per tile: cell of every point, the layout positions (a counting
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+  if (NT == 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
+// Cell layout of tile t by a group of NT threads (one warp, or the whole block
+// for a large tile): cell of every point, the layout positions (a counting
 // sort by cell inside the tile's range), cell ranges and member boxes, and the
-// density sweep's work order for the tile.
-template <int D>
-__global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a) {
+// density sweep's work order for the tile. cnt holds the tile's s^D cell
+// counters, ccnt box_classes<D>() class counters.
+template <int D, int NT>
+__device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, int* cnt, int* ccnt) {
   constexpr int E = box_classes<D>();
-  __shared__ int s_cnt[kCellWarps][kCellSlots];
-  __shared__ int s_cls[kCellWarps][E];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int* cnt = s_cnt[warp];
-  int* ccnt = s_cls[warp];
+  const int tid = NT == 32 ? (threadIdx.x & 31) : (int)threadIdx.x;
+  const int lane = threadIdx.x & 31;
   const int64_t n = a.n;
-  const int64_t stride = (int64_t)gridDim.x * kCellWarps;
-  for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
-    const int begin = a.tile_offset[t], end = a.tile_offset[t + 1];
-    const int m = end - begin;
-    if (m == 0)
-      continue;
-    const EventDesc ev = a.events[a.sevt[begin]];
-    const GridDesc& g = a.grids[ev.grid];
-    const int s = cells_per_dim<D>(m);
-    float lo[D], inv[D];
-    int own[D];
-    {
-      int local = (int)t - ev.tile_base;
+  group_sync<NT>();  // the previous tile of this group is done with cnt/ccnt
+  const int begin = a.tile_offset[t], end = a.tile_offset[t + 1];
+  const int m = end - begin;
+  if (m == 0)
+    return;
+  const EventDesc ev = a.events[a.sevt[begin]];
+  const GridDesc& g = a.grids[ev.grid];
+  const int s = cells_per_dim<D>(m);
+  float lo[D], inv[D];
+  int own[D];
+  {
+    int local = (int)t - ev.tile_base;
 #pragma unroll
-      for (int d = 0; d < D; ++d) {
-        own[d] = local / g.stride[d];
-        local -= own[d] * g.stride[d];
-        cell_axis(g, own[d], s, d, lo[d], inv[d]);
-      }
+    for (int d = 0; d < D; ++d) {
+      own[d] = local / g.stride[d];
+      local -= own[d] * g.stride[d];
+      cell_axis(g, own[d], s, d, lo[d], inv[d]);
     }
-    if (lane == 0) {
-      a.cell_s[t] = s;
-      if (D == 2) {
-        a.cell_geom[t] = make_float4(lo[0], lo[1], inv[0], inv[1]);
-      } else {
-        a.cell_geom[2 * t] = make_float4(lo[0], lo[1], lo[D - 1], inv[0]);
-        a.cell_geom[2 * t + 1] = make_float4(inv[1], inv[D - 1], 0.0f, 0.0f);
-      }
+  }
+  if (tid == 0) {
+    a.cell_s[t] = s;
+    if (D == 2) {
+      a.cell_geom[t] = make_float4(lo[0], lo[1], inv[0], inv[1]);
+    } else {
+      a.cell_geom[2 * t] = make_float4(lo[0], lo[1], lo[D - 1], inv[0]);
+      a.cell_geom[2 * t + 1] = make_float4(inv[1], inv[D - 1], 0.0f, 0.0f);
     }
-    const int S = D == 2 ? s * s : s * s * s;
-    for (int c = lane; c < S; c += 32)
-      cnt[c] = 0;
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) {
-      const int q = begin + i;
-      int c = 0;
+  }
+  const int S = D == 2 ? s * s : s * s * s;
+  for (int c = tid; c < S; c += NT)
+    cnt[c] = 0;
+  for (int c = tid; c < E; c += NT)
+    ccnt[c] = 0;
+  group_sync<NT>();
+  for (int i = tid; i < m; i += NT) {
+    const int q = begin + i;
+    int c = 0;
 #pragma unroll
-      for (int d = 0; d < D; ++d)
-        c = c * s + cell_coord(a.sx[d * n + q], lo[d], inv[d], s);
-      atomicAdd(&cnt[c], 1);
-      a.cell_slot[q] = begin + c;
-    }
-    __syncwarp();
+    for (int d = 0; d < D; ++d)
+      c = c * s + cell_coord(a.sx[d * n + q], lo[d], inv[d], s);
+    atomicAdd(&cnt[c], 1);
+    a.cell_slot[q] = begin + c;
+  }
+  group_sync<NT>();
+  if (tid < 32)
     warp_scan_range(cnt, S);
-    __syncwarp();
-    for (int c = lane; c < S; c += 32) {
-      CellInfo ci;
-      ci.start = begin + cnt[c];
-      ci.end = begin + (c + 1 < S ? cnt[c + 1] : m);
-      ci.maxkey = 0ull;
-      a.cell_info[begin + c] = ci;
+  group_sync<NT>();
+  for (int c = tid; c < S; c += NT) {
+    CellInfo ci;
+    ci.start = begin + cnt[c];
+    ci.end = begin + (c + 1 < S ? cnt[c + 1] : m);
+    ci.maxkey = 0ull;
+    a.cell_info[begin + c] = ci;
+  }
+  group_sync<NT>();
+  for (int i = tid; i < m; i += NT) {
+    const int q = begin + i;
+    const int pos = begin + atomicAdd(&cnt[a.cell_slot[q] - begin], 1);
+    a.nh_pos[q] = pos;
+    a.nh_q[pos] = q;
+  }
+  group_sync<NT>();
+  // Member boxes. A point with a NaN coordinate is never within reach and
+  // is left out; a cell without other members gets an empty box (+inf, -inf).
+  for (int c = tid; c < S; c += NT) {
+    const int c_end = c + 1 < S ? cnt[c] : m;  // cursors now hold the cell ends
+    const int c_begin = c > 0 ? cnt[c - 1] : 0;
+    float mn[D], mx[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      mn[d] = INFINITY;
+      mx[d] = -INFINITY;
     }
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) {
-      const int q = begin + i;
-      const int pos = begin + atomicAdd(&cnt[a.cell_slot[q] - begin], 1);
-      a.nh_pos[q] = pos;
-      a.nh_q[pos] = q;
-    }
-    __syncwarp();
-    // Member boxes. A point with a NaN coordinate is never within reach and
-    // is left out; a cell without other members gets an empty box (+inf, -inf).
-    for (int c = lane; c < S; c += 32) {
-      const int c_end = c + 1 < S ? cnt[c] : m;  // cursors now hold the cell ends
-      const int c_begin = c > 0 ? cnt[c - 1] : 0;
-      float mn[D], mx[D];
+    for (int k = c_begin; k < c_end; ++k) {
+      const int q = a.nh_q[begin + k];
+      float x[D];
+      bool ok = true;
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        mn[d] = INFINITY;
-        mx[d] = -INFINITY;
+        x[d] = a.sx[d * n + q];
+        ok &= x[d] == x[d];
       }
-      for (int k = c_begin; k < c_end; ++k) {
-        const int q = a.nh_q[begin + k];
-        float x[D];
-        bool ok = true;
+      if (ok) {
 #pragma unroll
         for (int d = 0; d < D; ++d) {
-          x[d] = a.sx[d * n + q];
-          ok &= x[d] == x[d];
-        }
-        if (ok) {
-#pragma unroll
-          for (int d = 0; d < D; ++d) {
-            mn[d] = fminf(mn[d], x[d]);
-            mx[d] = fmaxf(mx[d], x[d]);
-          }
+          mn[d] = fminf(mn[d], x[d]);
+          mx[d] = fmaxf(mx[d], x[d]);
         }
       }
-      if (D == 2) {
-        a.cell_box[begin + c] = make_float4(mn[0], mn[1], mx[0], mx[1]);
-      } else {
-        a.cell_box[2 * (begin + c)] = make_float4(mn[0], mn[1], mn[D - 1], mx[0]);
-        a.cell_box[2 * (begin + c) + 1] = make_float4(mx[1], mx[D - 1], 0.0f, 0.0f);
-      }
     }
-    __syncwarp();
-    // Density work order: the tile's points grouped by search-box class (the
-    // lanes of a warp share one box) and in cell-layout order inside a class
-    // (they are neighbours, so the cells within reach of the warp are few). A
-    // stable counting sort: rounds of 32 layout positions, in order, ranked
-    // within a round by __match_any_sync.
-    for (int c = lane; c < E; c += 32)
-      ccnt[c] = 0;
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) {
-      const int q = a.nh_q[begin + i];
-      float xq[D];
-      const float zero[3] = {0.0f, 0.0f, 0.0f};
+    if (D == 2) {
+      a.cell_box[begin + c] = make_float4(mn[0], mn[1], mx[0], mx[1]);
+    } else {
+      a.cell_box[2 * (begin + c)] = make_float4(mn[0], mn[1], mn[D - 1], mx[0]);
+      a.cell_box[2 * (begin + c) + 1] = make_float4(mx[1], mx[D - 1], 0.0f, 0.0f);
+    }
+  }
+  // Density work order: the tile's points grouped by search-box class (the
+  // lanes of a warp share one box) and in cell-layout order inside a class
+  // (they are neighbours). A counting sort by class: rounds of 32 layout
+  // positions per warp, grouped within a round by __match_any_sync; one warp
+  // keeps the layout order inside a class, several warps interleave their
+  // rounds (any order inside a class is correct: it only decides which lane
+  // computes which point).
+  for (int i = tid; i < m; i += NT) {
+    const int q = a.nh_q[begin + i];
+    float xq[D];
+    const float zero[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-      for (int d = 0; d < D; ++d)
-        xq[d] = a.sx[d * n + q];
-      int inf[D], sup[D];
-      search_box<D>(g, p, xq, zero, p.dc, inf, sup);
-      const int c = box_class<D>(g, own, inf, sup);
-      a.cls_dens[begin + i] = c;
-      atomicAdd(&ccnt[c], 1);
-    }
-    __syncwarp();
+    for (int d = 0; d < D; ++d)
+      xq[d] = a.sx[d * n + q];
+    int inf[D], sup[D];
+    search_box<D>(g, p, xq, zero, p.dc, inf, sup);
+    const int c = box_class<D>(g, own, inf, sup);
+    a.cls_dens[begin + i] = c;
+    atomicAdd(&ccnt[c], 1);
+  }
+  group_sync<NT>();
+  if (tid < 32)
     warp_scan_range(ccnt, E);
-    __syncwarp();
-    for (int base = 0; base < m; base += 32) {
-      const int i = base + lane;
-      const bool valid = i < m;
-      const int c = valid ? a.cls_dens[begin + i] : -1;
-      const unsigned grp = __match_any_sync(kFullMask, c);
-      const int leader = __ffs(grp) - 1;
-      int first = 0;
-      if (valid && lane == leader) {
-        first = ccnt[c];
-        ccnt[c] = first + __popc(grp);
-      }
-      first = __shfl_sync(kFullMask, first, leader);
-      if (valid)
-        a.work_dens[begin + first + __popc(grp & lane_mask_lt())] = a.nh_q[begin + i];
-      __syncwarp();
+  group_sync<NT>();
+  for (int base = 0; base < m; base += NT) {
+    const int i = base + tid;
+    const bool valid = i < m;
+    const int c = valid ? a.cls_dens[begin + i] : -1;
+    const unsigned grp = __match_any_sync(kFullMask, c);
+    const int leader = __ffs(grp) - 1;
+    int first = 0;
+    if (valid && lane == leader)
+      first = atomicAdd(&ccnt[c], __popc(grp));
+    first = __shfl_sync(kFullMask, first, leader);
+    if (valid)
+      a.work_dens[begin + first + __popc(grp & lane_mask_lt())] = a.nh_q[begin + i];
+  }
+}
+
+// Cell layouts of all tiles. Blocks [0, warp_blocks) give one warp to each
+// tile of at most kLargeTilePoints points; the other blocks take the larger
+// tiles, which the tile sort listed, one block each, so a dense tile of
+// thousands of points does not hold up the launch on one warp.
+constexpr int kWarpCellSlots = kLargeTilePoints / kCellTarget;  // s^D * 2 <= m <= 256
+template <int D>
+__global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a,
+                                                          int warp_blocks) {
+  constexpr int E = box_classes<D>();
+  static_assert(kWarpCellSlots * kCellWarps <= kCellSlots, "warp counters fit the block's");
+  __shared__ int s_cnt[kCellSlots];
+  __shared__ int s_cls[kCellWarps][E];
+  const int warp = threadIdx.x >> 5;
+  if ((int)blockIdx.x < warp_blocks) {
+    const int64_t stride = (int64_t)warp_blocks * kCellWarps;
+    for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
+      if (a.tile_offset[t + 1] - a.tile_offset[t] > kLargeTilePoints)
+        continue;
+      tile_cells<D, 32>(p, a, t, s_cnt + warp * kWarpCellSlots, s_cls[warp]);
     }
+  } else {
+    const int n_large = *a.large_count;
+    for (int k = (int)blockIdx.x - warp_blocks; k < n_large; k += (int)gridDim.x - warp_blocks)
+      tile_cells<D, kCellWarps * 32>(p, a, a.large_tiles[k], s_cnt, s_cls[0]);
   }
 }
 
@@ -1080,8 +1163,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunP
                                                                    const SweepArgs a) {
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_nh;
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n;
-       w += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int64_t n_items = (n + 31) / 32;
+  for (;;) {
+    // next item of 32 layout positions (work per point varies a lot: points
+    // in dense cells test many more candidates)
+    int64_t item = 0;
+    if (lane == 0)
+      item = atomicAdd(reinterpret_cast<unsigned*>(&a.queue[1]), 1u);
+    item = __shfl_sync(kFullMask, item, 0);
+    if (item >= n_items)
+      break;
+    const int64_t w = item * 32 + lane;
+    if (w >= n)
+      continue;
     const int pi = (int)w;
     const int s = a.nh_q[pi];
     const float4 ri = rec[pi];
@@ -1221,12 +1316,15 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
     count_launches(1);
   }
   if (a.nh_pos) {
-    const int cell_blocks =
+    const int warp_blocks =
         (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, 148 * 32));
+    // blocks for the large tiles: at most one per tile that can be large
+    const int large_blocks =
+        (int)std::max<int64_t>(1, std::min<int64_t>(a.n / (kLargeTilePoints + 1), 148 * 4));
     if (D == 2)
-      k_cells<2><<<cell_blocks, kCellWarps * 32, 0, st>>>(p, a);
+      k_cells<2><<<warp_blocks + large_blocks, kCellWarps * 32, 0, st>>>(p, a, warp_blocks);
     else
-      k_cells<3><<<cell_blocks, kCellWarps * 32, 0, st>>>(p, a);
+      k_cells<3><<<warp_blocks + large_blocks, kCellWarps * 32, 0, st>>>(p, a, warp_blocks);
     count_launches(1);
   }
   return cudaGetLastError();

@@ -27,6 +27,14 @@ struct SweepArgs {
   int32_t* work_nh;
   int32_t* cls_dens;  // scratch: box class per sorted position
   int32_t* cls_nh;
+  // Work queues of the fast-path sweeps: [0] density, [1] nearest higher;
+  // each counts the 32-point work items taken so far (k_pack_density resets
+  // both), so warps that finish early take the next item.
+  int32_t* queue;
+  // Tiles of more than 256 points (listed by the tile sort) and their count:
+  // k_cells gives each of them a whole block.
+  const int32_t* large_tiles;
+  const int32_t* large_count;
   // Packed candidate records of the fast path (D = 2 or 3).
   float4* rec_dens;  // {x, y, [z], v}: v = flat * w for the flat kernel, else w
   float4* rec_nh;    // D = 2: {x, y, rho, tag bits}; D = 3: {x, y, z, rho}
