@@ -196,6 +196,8 @@ def run_ours(args, world, rank, local):
     weights_d = torch.from_numpy(ev.weights).to(dev)
     pts = clue.PointsDevice(coords_d, weights_d, outputs=("cluster_index",))
     algo = clue.Clusterer(1.5, 5.0, 1.5, device=local)
+    # launch choices picked by the library's autotuner on this batch (results do not depend on them)
+    tuning = algo.autotune(pts, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=stream, reps=1)
 
     def step():
         algo.make_clusters(pts, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=stream,
@@ -235,6 +237,7 @@ def run_ours(args, world, rank, local):
     h = clue.PointsHost(pin(ev.coords), pin(ev.weights))
     h.cluster_index = pin(np.zeros(n_total, np.int32))
     algo_h = clue.Clusterer(1.5, 5.0, 1.5, device=local)
+    algo_h.set_tuning(**tuning)
     hstream = torch.cuda.Stream(device=dev)
     for _ in range(max(1, args.warmup // 2)):
         algo_h.make_clusters(h, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=hstream)
@@ -263,6 +266,7 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(CONFIG, points_per_step=int(points_all), events_per_step=len(sizes) * world,
+                       tuning=tuning,
                        parallelism=f"replicas x{world} (events sharded by rank, no collective)"),
         "e2e": {"value": e2e_value, "unit": "points/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(ev.coords.nbytes + ev.weights.nbytes),
@@ -326,6 +330,7 @@ def run_extras(args, ev, sizes, local, stream, hbm_peak):
     bw = torch.from_numpy(big.weights).to(dev)
     bp = clue.PointsDevice(bc, bw, outputs=("cluster_index",))
     algo1 = clue.Clusterer(1.5, 8.0, 2.0, device=local)
+    algo1.autotune(bp, stream=stream, reps=1)
     for _ in range(3):
         algo1.make_clusters(bp, stream=stream)
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

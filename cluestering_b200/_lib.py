@@ -60,6 +60,11 @@ class Points(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("density_union_x16_2d", C.c_int32), ("density_union_x16_3d", C.c_int32),
+                ("label_jump_rounds", C.c_int32)]
+
+
 class ServerProfile(C.Structure):
     _fields_ = [("ndim", C.c_int32), ("params", Params)]
 
@@ -102,6 +107,12 @@ SIGNATURES = {
     "clue_workspace_set_profiling": (C.c_int, [_P, C.c_int32]),
     "clue_workspace_stage_ms": (C.c_int, [_P, _P, C.c_int32]),
     "clue_workspace_kernel_launches": (C.c_int, [_P, _P]),
+    "clue_tuning_defaults": (C.c_int, [C.POINTER(Tuning)]),
+    "clue_workspace_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "clue_workspace_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "clue_workspace_autotune": (
+        C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P, C.c_int32, C.c_int32, _P, C.c_int32,
+                  C.POINTER(Tuning)]),
     "clue_make_clusters_device": (C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P]),
     "clue_make_clusters_host": (C.c_int, [_P, C.POINTER(Params), C.POINTER(Points), _P]),
     "clue_make_clusters_batched_device": (

@@ -426,6 +426,45 @@ class Clusterer:
         L.check(L.load().clue_workspace_bytes(self._workspace(), C.byref(b)))
         return b.value
 
+    def get_tuning(self) -> dict:
+        """Launch choices of this clusterer's workspace (see clue_tuning)."""
+        t = L.Tuning()
+        L.check(L.load().clue_workspace_get_tuning(self._workspace(), C.byref(t)))
+        return {name: getattr(t, name) for name, _ in L.Tuning._fields_}
+
+    def set_tuning(self, **fields) -> None:
+        """Changes launch choices; results do not depend on them."""
+        t = L.Tuning()
+        lib = L.load()
+        L.check(lib.clue_workspace_get_tuning(self._workspace(), C.byref(t)))
+        for name, value in fields.items():
+            if name not in dict(L.Tuning._fields_):
+                raise KeyError(name)
+            setattr(t, name, int(value))
+        L.check(lib.clue_workspace_set_tuning(self._workspace(), C.byref(t)))
+
+    def autotune(self, points, metric=None, kernel=None, *, batch_item_sizes: Sequence[int] | None = None,
+                 grid_mode: int = L.GRID_SHARED, stream=None, reps: int = 3) -> dict:
+        """Times make_clusters on these device points under candidate launch
+        choices and keeps the fastest for this clusterer (clue_workspace_autotune);
+        results are the same under every choice. Returns the chosen tuning."""
+        if not isinstance(points, PointsDevice):
+            raise TypeError("autotune runs on device points")
+        lib = L.load()
+        prm = self.params(metric, kernel)
+        pts = _points_struct(points)
+        st = self._stream_handle(stream, False)
+        t = L.Tuning()
+        if batch_item_sizes is None:
+            L.check(lib.clue_workspace_autotune(self._workspace(), C.byref(prm), C.byref(pts), None, 0, 0, st,
+                                                int(reps), C.byref(t)))
+        else:
+            sizes = np.ascontiguousarray(batch_item_sizes, dtype=np.uint32)
+            L.check(lib.clue_workspace_autotune(self._workspace(), C.byref(prm), C.byref(pts), sizes.ctypes.data,
+                                                len(sizes), grid_mode, st, int(reps), C.byref(t)))
+        points.clustered = True
+        return {name: getattr(t, name) for name, _ in L.Tuning._fields_}
+
     def kernel_launches(self) -> int:
         """CUDA kernels the last make_clusters enqueued."""
         k = C.c_int64()

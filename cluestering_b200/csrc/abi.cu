@@ -366,8 +366,21 @@ float sqrt_threshold(float r) {
   return x;
 }
 
-RunParams make_run_params(const clue_params* p, const clue_points* pts) {
+clue_tuning default_tuning() {
+  clue_tuning t{};
+  // Measured on B200: in 2-D a warp with two box shapes reads its own
+  // candidates about as fast as it streams a union a quarter larger; in 3-D
+  // the per-point reads of mixed warps are far slower than any union.
+  t.density_union_x16_2d = 20;
+  t.density_union_x16_3d = 1 << 20;
+  t.label_jump_rounds = -1;
+  return t;
+}
+
+RunParams make_run_params(const clue_params* p, const clue_points* pts, const clue_tuning& t) {
   RunParams r{};
+  r.union_x16 = pts->ndim == 3 ? t.density_union_x16_3d : t.density_union_x16_2d;
+  r.jump_rounds = t.label_jump_rounds;
   r.D = pts->ndim;
   r.dc = p->dc;
   r.rhoc = p->rhoc;
@@ -484,7 +497,7 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   io.is_seed = pts->is_seed;
   io.rho = pts->rho;
   io.nh = pts->nearest_higher;
-  const RunParams prm = make_run_params(params, pts);
+  const RunParams prm = make_run_params(params, pts, ws->tuning);
   reset_launch_count();
   if ((e = launch_run(sh, prm, io, ws->b, st, ws->profiling ? ws->marks : nullptr)) != cudaSuccess)
     return fail_cuda(e, "kernel launch");
@@ -648,6 +661,7 @@ clue_status clue_workspace_create(clue_workspace** out, int32_t device) {
     return fail_cuda(e, "cudaSetDevice");
   auto* ws = new clue_workspace();
   ws->device = device;
+  ws->tuning = default_tuning();
   if ((e = cudaEventCreateWithFlags(&ws->run_event, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&ws->staging_event, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaMallocHost((void**)&ws->info, sizeof(RunInfo))) != cudaSuccess) {
@@ -679,6 +693,31 @@ clue_status clue_workspace_destroy(clue_workspace* ws) {
     if (m)
       cudaEventDestroy(m);
   delete ws;
+  return CLUE_OK;
+}
+
+clue_status clue_tuning_defaults(clue_tuning* out) {
+  if (!out)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null output pointer");
+  *out = default_tuning();
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_get_tuning(const clue_workspace* ws, clue_tuning* out) {
+  if (!ws || !out)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  *out = ws->tuning;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tuning) {
+  if (!ws || !tuning)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  if (tuning->density_union_x16_2d < 0 || tuning->density_union_x16_3d < 0)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "union thresholds must be >= 0");
+  if (tuning->label_jump_rounds < -1 || tuning->label_jump_rounds > 4)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "label_jump_rounds must be in [-1, 4]");
+  ws->tuning = *tuning;
   return CLUE_OK;
 }
 
@@ -746,6 +785,88 @@ clue_status clue_make_clusters_device(clue_workspace* ws, const clue_params* par
     return check_points(points, true, params ? params->metric_kind : 0);
   const uint32_t size = (uint32_t)points->n;
   return run_device(ws, params, points, &size, 1, CLUE_GRID_PER_EVENT, (cudaStream_t)stream, 0);
+}
+
+clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* params,
+                                    const clue_points* points, const uint32_t* event_sizes,
+                                    int32_t n_events, int32_t grid_mode, void* stream,
+                                    int32_t reps, clue_tuning* chosen) {
+  if (!ws || !params || !points)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace, parameters and points are required");
+  if (event_sizes && n_events <= 0)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "n_events must be positive");
+  if (event_sizes && grid_mode != CLUE_GRID_SHARED && grid_mode != CLUE_GRID_PER_EVENT)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "unknown grid mode");
+  if (reps < 1 || reps > 100)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "reps must be in [1, 100]");
+  if (points->n <= 0)
+    return check_points(points, true, params->metric_kind);
+  const uint32_t one = (uint32_t)points->n;
+  const uint32_t* sizes = event_sizes ? event_sizes : &one;
+  const int32_t ne = event_sizes ? n_events : 1;
+  const int32_t gm = event_sizes ? grid_mode : CLUE_GRID_PER_EVENT;
+  const cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaSetDevice(ws->device);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "cudaSetDevice");
+  cudaEvent_t ev[2] = {};
+  for (auto& x : ev)
+    if ((e = cudaEventCreate(&x)) != cudaSuccess)
+      return fail_cuda(e, "cudaEventCreate");
+  const clue_tuning start = ws->tuning;
+  // Median device time of `reps` runs under t, after one warm-up run.
+  auto time_runs = [&](const clue_tuning& t, float* ms) -> clue_status {
+    ws->tuning = t;
+    clue_status s = run_device(ws, params, points, sizes, ne, gm, st, 0);
+    std::vector<float> v;
+    for (int r = 0; r < reps && s == CLUE_OK; ++r) {
+      cudaEventRecord(ev[0], st);
+      s = run_device(ws, params, points, sizes, ne, gm, st, 0);
+      cudaEventRecord(ev[1], st);
+      if (s == CLUE_OK && (s = wait_run(ws)) == CLUE_OK) {
+        float x = 0.0f;
+        if ((e = cudaEventElapsedTime(&x, ev[0], ev[1])) != cudaSuccess)
+          s = fail_cuda(e, "cudaEventElapsedTime");
+        v.push_back(x);
+      }
+    }
+    if (s == CLUE_OK) {
+      std::sort(v.begin(), v.end());
+      *ms = v[v.size() / 2];
+    }
+    return s;
+  };
+  clue_tuning best = start;
+  float best_ms = 0.0f;
+  clue_status s = time_runs(best, &best_ms);
+  // One field at a time, each candidate against the best so far.
+  auto try_field = [&](int32_t clue_tuning::*field, std::initializer_list<int32_t> values) {
+    const clue_tuning base = best;
+    for (int32_t v : values) {
+      if (s != CLUE_OK || v == base.*field)
+        continue;
+      clue_tuning t = base;
+      t.*field = v;
+      float ms = 0.0f;
+      s = time_runs(t, &ms);
+      if (s == CLUE_OK && ms < best_ms) {
+        best = t;
+        best_ms = ms;
+      }
+    }
+  };
+  // The union threshold matters on the packed 2-D/3-D path only.
+  if (points->ndim == 2)
+    try_field(&clue_tuning::density_union_x16_2d, {0, 12, 16, 20, 24, 32, 48, 1 << 20});
+  else if (points->ndim == 3)
+    try_field(&clue_tuning::density_union_x16_3d, {0, 16, 24, 32, 48, 64, 1 << 20});
+  try_field(&clue_tuning::label_jump_rounds, {0, 1, 2, 3, 4});
+  for (auto& x : ev)
+    cudaEventDestroy(x);
+  ws->tuning = s == CLUE_OK ? best : start;
+  if (s == CLUE_OK && chosen)
+    *chosen = best;
+  return s;
 }
 
 clue_status clue_make_clusters_host(clue_workspace* ws, const clue_params* params,

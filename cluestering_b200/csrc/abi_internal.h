@@ -32,6 +32,7 @@ struct clue_workspace {
   std::vector<clue_impl::EventDesc> last_events;
   const int32_t* last_labels = nullptr;  // device cluster ids of the last run
   int64_t last_launches = 0;             // kernels the last run enqueued
+  clue_tuning tuning{};                  // launch choices (set at creation to the defaults)
 };
 
 namespace clue_impl {
@@ -52,7 +53,8 @@ clue_status stage_inputs(clue_workspace* ws, const clue_points* h, clue_points* 
 clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st);
 clue_status wait_run(clue_workspace* ws);
 float sqrt_threshold(float r);
-RunParams make_run_params(const clue_params* p, const clue_points* pts);
+clue_tuning default_tuning();
+RunParams make_run_params(const clue_params* p, const clue_points* pts, const clue_tuning& t);
 // Lays the buffers of capacity `c` out from `base` (or only measures them when
 // base is null) and returns the bytes they span.
 size_t carve_buffers(DeviceBuffers* b, const Capacity& c, char* base);

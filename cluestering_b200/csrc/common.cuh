@@ -82,6 +82,13 @@ struct RunParams {
   // Nonzero when every exponent the kernel can see for an in-range pair
   // (distance <= dc) lies where clue_expf needs no special-case branch.
   int32_t exp_in_range;
+  // Density sweep, warps whose lanes have different search boxes: the warp
+  // streams the union of the boxes when the union holds at most
+  // union_x16 / 16 times the candidates of its lanes' largest own box, else
+  // each lane reads its own candidates (clue_tuning::density_union_x16_2d/3d).
+  int32_t union_x16;
+  // Pointer-jumping rounds before the label walk; -1: by size.
+  int32_t jump_rounds;
 };
 
 // ---------------------------------------------------------------------------

@@ -852,7 +852,10 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   CLUE_CHECK(scan(b.seed_flag, b.seed_rank, n, b.counters + 1, b, st));
   // Large runs first shorten every chain with whole-array jumping rounds, so
   // the per-point walks below take a few steps; small runs walk directly.
-  const int jump_rounds = n >= (int64_t)1 << 22 ? 3 : n >= (int64_t)1 << 18 ? 2 : 0;
+  const int jump_rounds = prm.jump_rounds >= 0                ? prm.jump_rounds
+                          : n >= (int64_t)1 << 22 ? 3
+                          : n >= (int64_t)1 << 18 ? 2
+                                                  : 0;
   for (int r = 0; r < jump_rounds; ++r) {
     k_jump<<<grid_for(n), kThreads, 0, st>>>(n, b.parent);
     CLUE_LAUNCHED();

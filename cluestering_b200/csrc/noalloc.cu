@@ -142,7 +142,7 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   io.is_seed = pts->is_seed;
   io.rho = pts->rho;
   io.nh = pts->nearest_higher;
-  if ((e = launch_run(sh, make_run_params(params, pts), io, b, st)) != cudaSuccess)
+  if ((e = launch_run(sh, make_run_params(params, pts, default_tuning()), io, b, st)) != cudaSuccess)
     return fail_cuda(e, "kernel launch");
   if (device_status &&
       (e = cudaMemcpyAsync(device_status, b.status, sizeof(uint32_t), cudaMemcpyDeviceToDevice,

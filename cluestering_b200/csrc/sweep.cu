@@ -604,17 +604,23 @@ __device__ __forceinline__ void stream_issue(float4 (*ring)[kChunk], const int* 
   cp_async_commit();
 }
 
-// One streamed chunk for the kernels with an exponential (Gaussian,
-// exponential). The lanes of a warp seldom have the same candidates in range,
-// so evaluating the kernel inside the candidate loop would run it whenever any
-// lane is in range. Each lane first marks its in-range records of the chunk,
-// then evaluates the kernel on its own marked records only, lowest first: the
-// same additions in the same order as density_add_packed.
+// One streamed chunk through masks: each lane marks the records of the chunk
+// that are in range and in its own search box (`acc`: a warp streaming the
+// union of its lanes' boxes passes each lane the positions of its own box;
+// all ones when the boxes are equal), then adds its marked records lowest
+// first: the same additions in the same order as density_add_packed. For the
+// kernels with an exponential this also evaluates the kernel only on the
+// records the lane takes: the lanes of a warp seldom have the same candidates
+// in range, and a kernel evaluated inside the candidate loop would run
+// whenever any lane is in range.
 template <int D, int KIND>
 __device__ __forceinline__ void density_chunk_masked(const RunParams& p, unsigned long long xi_xy,
                                                      float zi, const ulonglong2* chunk, int cnt,
-                                                     int jself, float& rho) {
+                                                     unsigned acc, int jself, float wi,
+                                                     float& rho) {
   static_assert(kChunk == 32, "one mask bit per record of a chunk");
+  if (acc == 0)
+    return;
   unsigned m = 0;
   if (cnt == kChunk) {
 #pragma unroll 8
@@ -630,14 +636,24 @@ __device__ __forceinline__ void density_chunk_masked(const RunParams& p, unsigne
         m |= 1u << j;
     }
   }
+  m &= acc;
   while (m) {
     const int j = __ffs(m) - 1;
     m &= m - 1;
     float v;
     const float d2 = packed_d2<D>(xi_xy, zi, chunk[j], v);
-    const float k = kernel_value_in_range(p, __fsqrt_rn(d2), j == jself);
-    rho = __fadd_rn(rho, __fmul_rn(k, v));
+    if (KIND == CLUE_KERNEL_FLAT) {
+      rho = __fadd_rn(rho, j == jself ? wi : v);
+    } else {
+      const float k = kernel_value_in_range(p, __fsqrt_rn(d2), j == jself);
+      rho = __fadd_rn(rho, __fmul_rn(k, v));
+    }
   }
+}
+
+// Bits [lo, hi) of a 32-bit mask, 0 <= lo < hi <= 32.
+__device__ __forceinline__ unsigned range_bits(int lo, int hi) {
+  return (hi - lo == 32 ? 0xffffffffu : ((1u << (hi - lo)) - 1u)) << lo;
 }
 
 // Local density, one point per lane. When the 32 lanes of a warp share one
@@ -682,31 +698,54 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
     const float wi = a.sw[s];
     int inf[D], sup[D];
     search_box<D>(g, p, xi, zero, p.dc, inf, sup);
-    // one box for the whole warp?
-    bool same = __shfl_sync(kFullMask, ev.tile_base, 0) == ev.tile_base;
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      const int inf0 = __shfl_sync(kFullMask, inf[d], 0);
-      const int sup0 = __shfl_sync(kFullMask, sup[d], 0);
-      same &= (inf0 == inf[d]) & (sup0 == sup[d]);
-    }
     bool ordered = true;
 #pragma unroll
     for (int d = 0; d < D; ++d)
       ordered &= inf[d] <= sup[d];
-    const int n1 = D == 3 ? sup[1] - inf[1] + 1 : 1;
-    const int rows = ordered ? (sup[0] - inf[0] + 1) * n1 : 0;
+    // The warp's stream is the union U of its lanes' boxes (lanes of one event
+    // grid only). Each lane's box is a sub-box of U, and the reference's order
+    // over U restricted to a sub-box is the sub-box's own order, so every lane
+    // takes its own candidates from the shared stream in its own order.
+    const bool one_grid =
+        __all_sync(kFullMask, __shfl_sync(kFullMask, ev.tile_base, 0) == ev.tile_base);
+    int uinf[D], usup[D];
+    bool same = ordered, u_ordered = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      uinf[d] = __reduce_min_sync(kFullMask, ordered ? inf[d] : INT_MAX);
+      usup[d] = __reduce_max_sync(kFullMask, ordered ? sup[d] : INT_MIN);
+      same &= (inf[d] == uinf[d]) & (sup[d] == usup[d]);
+      u_ordered &= uinf[d] <= usup[d];
+    }
+    const bool uniform = __all_sync(kFullMask, same);
+    const int64_t n1 = (D == 3 && u_ordered) ? (int64_t)usup[1] - uinf[1] + 1 : 1;
+    const int64_t rows64 = u_ordered ? ((int64_t)usup[0] - uinf[0] + 1) * n1 : 0;
+    // U-row index of (b0, b1) (row table in off/qa) and this lane's part of
+    // that row as stream positions
+    auto u_row = [&](int b0, int b1) {
+      return (b0 - uinf[0]) * (int)n1 + (D == 3 ? b1 - uinf[1] : 0);
+    };
+    auto lane_part = [&](int b0, int b1, int& lo, int& hi) {
+      const int r = u_row(b0, b1);
+      int row = ev.tile_base + b0 * g.stride[0];
+      if (D == 3)
+        row += b1 * g.stride[1];
+      lo = off[r] + (a.tile_offset[row + inf[D - 1]] - qa[r]);
+      hi = off[r] + (a.tile_offset[row + sup[D - 1] + 1] - qa[r]);
+    };
     float rho = 0.0f;
-    if (__all_sync(kFullMask, same) && rows >= 1 && rows <= kMaxRows) {
-      // row table: lane r holds row r
+    bool streamed = false;  // warp-uniform
+    if (one_grid && rows64 >= 1 && rows64 <= kMaxRows) {
+      const int rows = (int)rows64;
+      // row table: lane r holds row r of U
       int len = 0, start = 0;
       if (lane < rows) {
-        const int b0 = inf[0] + lane / n1;
+        const int b0 = uinf[0] + lane / (int)n1;
         int row = ev.tile_base + b0 * g.stride[0];
         if (D == 3)
-          row += (inf[1] + lane % n1) * g.stride[1];
-        start = a.tile_offset[row + inf[D - 1]];
-        len = a.tile_offset[row + sup[D - 1] + 1] - start;
+          row += (uinf[1] + lane % (int)n1) * g.stride[1];
+        start = a.tile_offset[row + uinf[D - 1]];
+        len = a.tile_offset[row + usup[D - 1] + 1] - start;
       }
       int incl = len;
 #pragma unroll
@@ -723,22 +762,48 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
       if (lane == 0)
         off[rows] = total;
       __syncwarp();
+      // Lanes with different boxes: every lane pays for the whole union, so
+      // the union is streamed only while it is not much larger than the
+      // largest own box; otherwise each lane reads its own candidates below.
+      if (!uniform) {
+        int own_len = 0;
+        if (ordered)
+          for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
+            for (int b1 = D == 3 ? inf[1] : 0; b1 <= (D == 3 ? sup[1] : 0); ++b1) {
+              int lo, hi;
+              lane_part(b0, b1, lo, hi);
+              own_len += hi - lo;
+            }
+        const int max_own = __reduce_max_sync(kFullMask, own_len);
+        streamed = (int64_t)total * 16 <= (int64_t)p.union_x16 * max_own;
+      } else {
+        streamed = true;
+      }
+    }
+    if (streamed) {
+      const int rows = (int)rows64;
+      const int total = off[rows];
       // stream position of the point itself (its own tile is in the box unless
       // get_bin's clamping left it out)
       int p_self = -1;
       {
         int own[D];
-        bool in = true;
+        bool in = ordered;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
           own[d] = get_bin(g, p, xi[d], d);
           in &= inf[d] <= own[d] && own[d] <= sup[d];
         }
         if (in) {
-          const int r = (own[0] - inf[0]) * n1 + (D == 3 ? own[1] - inf[1] : 0);
+          const int r = u_row(own[0], D == 3 ? own[1] : 0);
           p_self = off[r] + (s - qa[r]);
         }
       }
+      // cursor over this lane's rows of U (last dimension excluded): the
+      // current row (cb0, cb1) and its stream positions [ilo, ihi)
+      int cb0 = inf[0], cb1 = D == 3 ? inf[1] : 0, ilo = INT_MAX, ihi = INT_MAX;
+      if (!uniform && ordered)
+        lane_part(cb0, cb1, ilo, ihi);
       const int chunks = (total + kChunk - 1) / kChunk;
       const unsigned long long xi_xy = pack2(xi[0], xi[1]);
       int rr = 0;  // row cursor of this lane's copies
@@ -750,27 +815,54 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
         cp_async_wait<kRing - 1>();
         __syncwarp();
         const ulonglong2* chunk = reinterpret_cast<const ulonglong2*>(ring[c % kRing]);
-        const int cnt = min(kChunk, total - c * kChunk);
-        const int jself = p_self - c * kChunk;  // own record's place in this chunk, if any
-        if (KIND != CLUE_KERNEL_FLAT) {
-          density_chunk_masked<D, KIND>(p, xi_xy, xi[2], chunk, cnt, jself, rho);
-        } else if (cnt == kChunk) {
+        const int base = c * kChunk;
+        const int cnt = min(kChunk, total - base);
+        const int jself = p_self - base;  // own record's place in this chunk, if any
+        if (uniform) {
+          if (KIND != CLUE_KERNEL_FLAT) {
+            density_chunk_masked<D, KIND>(p, xi_xy, xi[2], chunk, cnt, 0xffffffffu, jself, wi, rho);
+          } else if (cnt == kChunk) {
 #pragma unroll 8
-          for (int j = 0; j < kChunk; ++j)
-            density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
+            for (int j = 0; j < kChunk; ++j)
+              density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
+          } else {
+            for (int j = 0; j < cnt; ++j)
+              density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
+          }
         } else {
-          for (int j = 0; j < cnt; ++j)
-            density_add_packed<D, KIND>(p, xi_xy, xi[2], chunk[j], j == jself, wi, rho);
+          // positions of this chunk inside this lane's box
+          const int cend = base + cnt;
+          unsigned acc = 0;
+          while (ilo < cend) {
+            const int lo = max(ilo, base), hi = min(ihi, cend);
+            if (lo < hi)
+              acc |= range_bits(lo - base, hi - base);
+            if (ihi > cend)
+              break;  // the row goes on in the next chunk
+            // next row of this lane's box
+            if (D == 3 && cb1 < sup[1]) {
+              ++cb1;
+            } else {
+              cb1 = D == 3 ? inf[1] : 0;
+              ++cb0;
+            }
+            if (cb0 > sup[0]) {
+              ilo = ihi = INT_MAX;
+              break;
+            }
+            lane_part(cb0, cb1, ilo, ihi);
+          }
+          density_chunk_masked<D, KIND>(p, xi_xy, xi[2], chunk, cnt, acc, jself, wi, rho);
         }
         __syncwarp();
       }
       cp_async_wait<0>();
       __syncwarp();
-    } else {
+    }
+    if (!streamed)
       for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
         density_add<D, KIND>(p, xi, __ldg(&rec[q]), q == s, wi, rho);
       });
-    }
     if (!active)
       continue;
     a.srho[s] = rho;

@@ -154,6 +154,43 @@ clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t
  * counterpart; a check that the run executed on the GPU). */
 clue_status clue_workspace_kernel_launches(const clue_workspace* ws, int64_t* launches);
 
+/* ---- launch tuning (no counterpart in the reference, whose alpaka work
+ * division is fixed at compile time). None of these choices changes a result:
+ * they decide only how the work is spread over the GPU. ------------------- */
+typedef struct {
+  /* Density sweep, 2-D and 3-D Euclidean runs: a warp whose 32 points have
+   * different search boxes streams the union of their boxes through shared
+   * memory when the union holds at most (threshold / 16) times the
+   * candidates of the warp's largest own box; otherwise each point reads its
+   * own candidates from global memory. 0 never streams such warps; a large
+   * value (>= 1 << 20) always does. One value for 2-D runs, one for 3-D. */
+  int32_t density_union_x16_2d;
+  int32_t density_union_x16_3d;
+  /* Labels: whole-array pointer-jumping rounds over the follower tree before
+   * each point walks to its seed (0..4); -1 picks by size (none below 2^18
+   * points, 2 below 2^22, else 3). */
+  int32_t label_jump_rounds;
+} clue_tuning;
+
+/* Defaults: the values the library ships with. */
+clue_status clue_tuning_defaults(clue_tuning* out);
+/* The workspace's current choices (defaults until set or autotuned). */
+clue_status clue_workspace_get_tuning(const clue_workspace* ws, clue_tuning* out);
+/* CLUE_ERR_INVALID_ARGUMENT if a field is out of range (a negative threshold,
+ * jump rounds outside -1..4). */
+clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tuning);
+/* Autotuner: runs make_clusters on these device points (the single-event form
+ * when event_sizes is NULL, else the batched form with grid_mode) under
+ * candidate tunings, one field at a time, times each candidate with CUDA events
+ * on `stream` (median of `reps` runs after one warm-up run), keeps the fastest
+ * in the workspace and returns it in *chosen (may be NULL). The points' outputs
+ * are written by every run and hold the (unchanged) result at the end. Blocks
+ * until done. */
+clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* params,
+                                    const clue_points* points, const uint32_t* event_sizes,
+                                    int32_t n_events, int32_t grid_mode, void* stream,
+                                    int32_t reps, clue_tuning* chosen);
+
 /* ---- clustering ----------------------------------------------------------- */
 /* Clusterer::make_clusters(Queue&, PointsDevice&, metric, kernel)
  * (core/detail/Clusterer.hpp:139-151). Device pointers; asynchronous. */

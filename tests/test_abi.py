@@ -117,3 +117,12 @@ def test_clusters_csr_host():
     offs, pts = clue.clusters_csr(np.array([1, -1, 0, 1, 0, 2], np.int32))
     assert offs.tolist() == [0, 2, 4, 5]
     assert pts.tolist() == [2, 4, 0, 3, 5]
+
+
+def test_tuning_defaults_and_struct_layout():
+    t = L.Tuning()
+    assert L.load().clue_tuning_defaults(C.byref(t)) == 0
+    # 2-D mixed warps stream unions up to 1.25x; 3-D always streams; jump rounds by size
+    assert (t.density_union_x16_2d, t.density_union_x16_3d, t.label_jump_rounds) == (20, 1 << 20, -1)
+    assert C.sizeof(L.Tuning) == 12
+    assert L.load().clue_tuning_defaults(None) == L.ERR_INVALID_ARGUMENT

@@ -372,3 +372,66 @@ def test_host_and_device_entry_points_agree():
     for k in ("rho", "nh", "seed", "ci"):
         assert np.array_equal(a[k], b[k])
     assert same_partition(a["ci"], b["ci"])
+
+
+# ---- launch tuning: results must not depend on it ---------------------------------------------
+
+TUNINGS = [
+    dict(density_union_x16_2d=0, density_union_x16_3d=0, label_jump_rounds=0),
+    dict(density_union_x16_2d=1 << 20, density_union_x16_3d=1 << 20, label_jump_rounds=4),
+    dict(density_union_x16_2d=16, density_union_x16_3d=24, label_jump_rounds=1),
+]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS)
+def test_results_do_not_depend_on_tuning_2d(tuning):
+    ev, sizes = W.batch_2d(48, 256, 16384, seed=31)
+    w = np.random.default_rng(5).exponential(1.0, ev.n).astype(np.float32)
+    c = clue.Clusterer(1.5, 5.0, 1.5)
+    c.set_tuning(**tuning)
+    assert c.get_tuning() == tuning
+    check(ev.coords, w, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT, clusterer=c)
+
+
+@pytest.mark.parametrize("tuning", TUNINGS)
+def test_results_do_not_depend_on_tuning_3d_showers(tuning):
+    # dense showers: most density warps mix search boxes and stream their union
+    ev = W.layered_3d(40000, seed=12)
+    c = clue.Clusterer(3.0, 10.0, 4.0)
+    c.set_tuning(**tuning)
+    check(ev.coords, ev.weights, 3.0, 10.0, 4.0, kernel="gaussian", kernel_params=(1.0, 1.0),
+          clusterer=c, path="device")
+
+
+def test_set_tuning_rejects_out_of_range():
+    c = clue.Clusterer(1.5, 5.0, 1.5)
+    with pytest.raises(ValueError):
+        c.set_tuning(density_union_x16_2d=-1)
+    with pytest.raises(ValueError):
+        c.set_tuning(label_jump_rounds=5)
+    with pytest.raises(KeyError):
+        c.set_tuning(points_per_tile=64)
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_autotune_keeps_results(batched):
+    import torch
+    dev = torch.device("cuda:0")
+    if batched:
+        ev, sizes = W.batch_2d(64, 256, 8192, seed=41)
+        prm = (1.5, 5.0, 1.5)
+        kern = clue.FlatKernel(0.5)
+    else:
+        ev, sizes = W.layered_3d(20000, seed=13), None
+        prm = (3.0, 10.0, 4.0)
+        kern = clue.GaussianKernel(1.0, 1.0)
+    pts = clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev))
+    c = clue.Clusterer(*prm)
+    chosen = c.autotune(pts, clue.EuclideanMetric(), kern, batch_item_sizes=sizes,
+                        grid_mode=clue.GRID_PER_EVENT, reps=1)
+    assert c.get_tuning() == chosen
+    o = run_oracle(ev.coords, ev.weights, *prm, kernel="flat" if batched else "gaussian",
+                   kernel_params=(0.5,) if batched else (1.0, 1.0), sizes=sizes,
+                   grid_mode=clue.GRID_PER_EVENT)
+    assert_identical(dict(rho=pts.rho.cpu().numpy(), nh=pts.nearest_higher.cpu().numpy(),
+                          seed=pts.is_seed.cpu().numpy(), ci=pts.cluster_index.cpu().numpy()), o)
