@@ -379,13 +379,22 @@ def run_serving(args, local):
     total = sum(ev.n for ev in evs)
     cfg = dict(device=local, budget_bytes=40 << 30, max_inflight=args.serve_inflight,
                max_batch_events=args.serve_batch_events, max_batch_points=args.serve_batch_points,
-               linger_us=args.serve_linger_us)
+               linger_us=args.serve_linger_us, max_batch_ms=args.serve_batch_ms,
+               priority_ms=args.serve_priority_ms)
     out = {"events": len(evs), "points": total, "mix": "80% 2-D single_2d-style, 20% 3-D layered_3d-style",
-           "sizes": "log-uniform [1024, 262144]", "config": cfg}
-    with clue.Server(profs, **cfg) as srv:
-        for i in range(min(32, len(evs))):  # warm-up
+           "sizes": "log-uniform [1024, 262144]", "config": cfg, "stream": args.serve_stream,
+           "method": "each server first clusters 64 events (not counted), which also seeds its cost "
+                     "model; peak = all events submitted at once; loads = a Poisson stream of "
+                     "`stream` arrivals cycling through the events"}
+    warm = min(64, len(evs))
+
+    def warm_up(srv):
+        for i in range(warm):
             srv.submit(prof_of[i], pts[i])
         srv.drain()
+
+    with clue.Server(profs, **cfg) as srv:
+        warm_up(srv)
         t0 = time.perf_counter()
         for i, p in enumerate(pts):
             srv.submit(prof_of[i], p)
@@ -393,23 +402,28 @@ def run_serving(args, local):
         peak = total / (time.perf_counter() - t0)
     out["peak_points_per_s"] = peak
     peak_events = peak / (total / len(evs))
+    # arrival k is event k mod len(evs); repeats of one event are len(evs) arrivals
+    # apart, long after the earlier one completed at these loads
+    order = [k % len(evs) for k in range(args.serve_stream)]
+    stream_points = sum(evs[i].n for i in order)
     loads = []
     rng = np.random.default_rng(0)
     for f in args.serve_loads:
         with clue.Server(profs, **cfg) as srv:
-            gaps = rng.exponential(1.0 / (f * peak_events), size=len(evs))
+            warm_up(srv)
+            gaps = rng.exponential(1.0 / (f * peak_events), size=len(order))
             t_next = time.perf_counter()
             t0 = t_next
-            for i, p in enumerate(pts):
-                t_next += gaps[i]
+            for k, i in enumerate(order):
+                t_next += gaps[k]
                 while time.perf_counter() < t_next:
                     pass
-                srv.submit(prof_of[i], p)
+                srv.submit(prof_of[i], pts[i])
             srv.drain()
             dt = time.perf_counter() - t0
-            lat = srv.latencies_ms()
+            lat = srv.latencies_ms()[warm:]
             st = srv.stats()
-        loads.append({"load": f, "points_per_s": total / dt, "p50_ms": float(np.percentile(lat, 50)),
+        loads.append({"load": f, "points_per_s": stream_points / dt, "p50_ms": float(np.percentile(lat, 50)),
                       "p99_ms": float(np.percentile(lat, 99)), "batches": st["batches"]})
     out["loads"] = loads
     half = min(loads, key=lambda r: abs(r["load"] - 0.5))
@@ -465,6 +479,9 @@ def main():
     ap.add_argument("--serve-batch-events", type=int, default=64)
     ap.add_argument("--serve-batch-points", type=int, default=2_000_000)
     ap.add_argument("--serve-linger-us", type=int, default=200)
+    ap.add_argument("--serve-batch-ms", type=float, default=2.0)
+    ap.add_argument("--serve-priority-ms", type=float, default=1.5)
+    ap.add_argument("--serve-stream", type=int, default=4000)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--skip-extras", action="store_true")
     ap.add_argument("--case", choices=["one-tile"], default=None,

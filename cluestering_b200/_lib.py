@@ -77,6 +77,8 @@ class ServerConfig(C.Structure):
         ("max_batch_events", C.c_int32),
         ("max_batch_points", C.c_int64),
         ("linger_us", C.c_int32),
+        ("max_batch_ms", C.c_float),
+        ("priority_ms", C.c_float),
     ]
 
 

@@ -487,7 +487,8 @@ class Server:
     """
 
     def __init__(self, profiles, *, device: int = 0, budget_bytes: int = 8 << 30, max_inflight: int = 4,
-                 max_batch_events: int = 1024, max_batch_points: int = 0, linger_us: int = 200):
+                 max_batch_events: int = 1024, max_batch_points: int = 0, linger_us: int = 200,
+                 max_batch_ms: float = 0.0, priority_ms: float = 0.0):
         lib = L.load()
         arr = (L.ServerProfile * len(profiles))()
         for i, (ndim, clusterer, metric, kernel) in enumerate(profiles):
@@ -495,7 +496,7 @@ class Server:
             arr[i].params = clusterer.params(metric, kernel)
         cfg = L.ServerConfig(device=device, budget_bytes=budget_bytes, max_inflight=max_inflight,
                              max_batch_events=max_batch_events, max_batch_points=max_batch_points,
-                             linger_us=linger_us)
+                             linger_us=linger_us, max_batch_ms=max_batch_ms, priority_ms=priority_ms)
         h = C.c_void_p()
         L.check(lib.clue_server_create(C.byref(h), C.byref(cfg), arr, len(profiles)))
         self._h = h

@@ -69,7 +69,11 @@ int bucket_of(int32_t n) {
 }  // namespace
 
 struct Slot {
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;     // default priority
+  cudaStream_t stream_hi = nullptr;  // highest priority: batches holding a long event
+  cudaStream_t active = nullptr;     // the stream of the batch in flight
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;  // device time of the batch
+  int32_t profile = 0;
   clue_workspace* ws = nullptr;
   // device inputs and outputs of one batch (planes of max_points)
   float* d_coords = nullptr;
@@ -96,6 +100,9 @@ struct Slot {
 struct clue_server {
   clue_server_config cfg;
   std::vector<clue_server_profile> profiles;
+  // Device time per point of each profile (ns), learned from finished batches
+  // of at least kCostSamplePoints points; 0 until the first such batch.
+  std::vector<double> ns_per_point;
   int32_t max_dim = 1;
   int64_t max_points = 0;
   std::vector<Slot*> slots;
@@ -146,15 +153,36 @@ int64_t pending_points(clue_server* srv, int profile) {
   return n;
 }
 
+// Batches of fewer points have their time dominated by per-launch latency and
+// are not used to learn the per-point cost.
+constexpr int64_t kCostSamplePoints = 1 << 16;
+
+int64_t pending_points(clue_server* srv, int profile);
+
+// Points a batch of `profile` may hold: the memory cap, and the time cap once
+// the profile's cost per point is known (at least one event always goes in).
+// The time cap grows with the backlog: when the pending work of the profile
+// exceeds what the slots clear in batches of max_batch_ms, queueing dominates
+// the latency and larger batches (fewer per-batch overheads) clear it sooner.
+int64_t batch_point_cap(clue_server* srv, int profile) {
+  const double ns = srv->ns_per_point[profile];
+  if (srv->cfg.max_batch_ms <= 0.0f || ns <= 0.0)
+    return srv->max_points;
+  const double backlog_ms = (double)pending_points(srv, profile) * ns * 1e-6;
+  const double cap_ms = std::max<double>(srv->cfg.max_batch_ms, backlog_ms / srv->cfg.max_inflight);
+  return std::min<int64_t>(srv->max_points, (int64_t)(cap_ms * 1e6 / ns));
+}
+
 // Takes a batch for `profile` starting from `bucket`, then smaller buckets.
 std::vector<Request> take_batch(clue_server* srv, int profile, int bucket) {
   std::vector<Request> out;
   int64_t pts = 0;
+  const int64_t cap = batch_point_cap(srv, profile);
   auto& qs = srv->queues[profile];
   for (auto it = qs.find(bucket);; --it) {
     auto& q = it->second;
     while (!q.empty() && (int)out.size() < srv->cfg.max_batch_events &&
-           pts + q.front().pts.n <= srv->max_points) {
+           pts + q.front().pts.n <= srv->max_points && (out.empty() || pts + q.front().pts.n <= cap)) {
       pts += q.front().pts.n;
       out.push_back(q.front());
       q.pop_front();
@@ -179,6 +207,17 @@ clue_status launch_batch(clue_server* srv, Slot* s, std::vector<Request>&& reqs)
   const int64_t P = s->offsets[B];
   bool want_seed = false, want_rho = false, want_nh = false;
   cudaError_t e;
+  // A batch holding an event that is expected to run long goes first on the GPU.
+  int32_t n_max = 0;
+  for (uint32_t z : sizes)
+    n_max = std::max<int32_t>(n_max, (int32_t)z);
+  const double ns = srv->ns_per_point[s->batch[0].profile];
+  const bool urgent = srv->cfg.priority_ms > 0.0f && ns > 0.0 &&
+                      (double)n_max * ns * 1e-6 >= srv->cfg.priority_ms;
+  s->active = urgent ? s->stream_hi : s->stream;
+  s->profile = s->batch[0].profile;
+  if ((e = cudaEventRecord(s->ev_start, s->active)))
+    return fail_cuda(e, "batch start event");
   for (int k = 0; k < B; ++k) {
     const Request& r = s->batch[k];
     const int64_t off = s->offsets[k];
@@ -190,7 +229,7 @@ clue_status launch_batch(clue_server* srv, Slot* s, std::vector<Request>&& reqs)
       const float* src = d < D ? r.pts.coords[d] : r.pts.weight;
       float* dst_dev = d < D ? s->d_coords + d * P + off : s->d_weight + off;
       if (r.pinned) {
-        if ((e = cudaMemcpyAsync(dst_dev, src, nb, cudaMemcpyHostToDevice, s->stream)))
+        if ((e = cudaMemcpyAsync(dst_dev, src, nb, cudaMemcpyHostToDevice, s->active)))
           return fail_cuda(e, "event upload");
       } else {
         float* dst_host = d < D ? s->h_coords + d * P + off : s->h_weight + off;
@@ -212,7 +251,7 @@ clue_status launch_batch(clue_server* srv, Slot* s, std::vector<Request>&& reqs)
       for (int d = 0; d <= D; ++d) {
         float* dst_dev = d < D ? s->d_coords + d * P + off : s->d_weight + off;
         const float* src = d < D ? s->h_coords + d * P + off : s->h_weight + off;
-        if ((e = cudaMemcpyAsync(dst_dev, src, nb, cudaMemcpyHostToDevice, s->stream)))
+        if ((e = cudaMemcpyAsync(dst_dev, src, nb, cudaMemcpyHostToDevice, s->active)))
           return fail_cuda(e, "event upload");
       }
     }
@@ -227,10 +266,10 @@ clue_status launch_batch(clue_server* srv, Slot* s, std::vector<Request>&& reqs)
   dev.rho = want_rho ? s->d_rho : nullptr;
   dev.nearest_higher = want_nh ? s->d_nh : nullptr;
   clue_status st = run_device(s->ws, &prof.params, &dev, sizes.data(), B, CLUE_GRID_PER_EVENT,
-                              s->stream, 0);
+                              s->active, 0);
   if (st != CLUE_OK)
     return st;
-  if ((e = launch_localize(s->ws->b, B, P, s->d_cluster, want_nh ? s->d_nh : nullptr, s->stream)))
+  if ((e = launch_localize(s->ws->b, B, P, s->d_cluster, want_nh ? s->d_nh : nullptr, s->active)))
     return fail_cuda(e, "relabel");
   for (int k = 0; k < B; ++k) {
     const Request& r = s->batch[k];
@@ -248,12 +287,14 @@ clue_status launch_batch(clue_server* srv, Slot* s, std::vector<Request>&& reqs)
       if (!o.user)
         continue;
       void* dst = r.pinned ? o.user : o.staging;
-      if ((e = cudaMemcpyAsync(dst, o.dev, nb, cudaMemcpyDeviceToHost, s->stream)))
+      if ((e = cudaMemcpyAsync(dst, o.dev, nb, cudaMemcpyDeviceToHost, s->active)))
         return fail_cuda(e, "result download");
     }
   }
+  if ((e = cudaEventRecord(s->ev_end, s->active)))
+    return fail_cuda(e, "batch end event");
   s->done.store(false);
-  if ((e = cudaLaunchHostFunc(s->stream, on_batch_done, s)))
+  if ((e = cudaLaunchHostFunc(s->active, on_batch_done, s)))
     return fail_cuda(e, "completion callback");
   return CLUE_OK;
 }
@@ -261,6 +302,12 @@ clue_status launch_batch(clue_server* srv, Slot* s, std::vector<Request>&& reqs)
 // Copies staged outputs of pageable requests back and completes the tickets.
 void retire_batch(clue_server* srv, Slot* s, bool ok) {
   const double t = now_s();
+  int64_t P = 0;
+  for (auto& r : s->batch)
+    P += r.pts.n;
+  float ms = 0.0f;
+  const bool timed = ok && P >= kCostSamplePoints &&
+                     cudaEventElapsedTime(&ms, s->ev_start, s->ev_end) == cudaSuccess;
   for (size_t k = 0; k < s->batch.size(); ++k) {
     const Request& r = s->batch[k];
     if (ok && !r.pinned) {
@@ -276,6 +323,11 @@ void retire_batch(clue_server* srv, Slot* s, bool ok) {
     }
   }
   std::lock_guard<std::mutex> lock(srv->mu);
+  if (timed) {
+    double& ns = srv->ns_per_point[s->profile];
+    const double sample = (double)ms * 1e6 / (double)P;
+    ns = ns > 0.0 ? 0.8 * ns + 0.2 * sample : sample;
+  }
   for (auto& r : s->batch) {
     srv->state[r.ticket] = ok ? kDone : kFailed;
     srv->t_done[r.ticket] = t;
@@ -296,7 +348,7 @@ void scheduler_loop(clue_server* srv) {
     for (Slot* s : srv->slots)
       if (s->busy && s->done.load()) {
         lock.unlock();
-        const bool ok = cudaStreamSynchronize(s->stream) == cudaSuccess;
+        const bool ok = cudaStreamSynchronize(s->active) == cudaSuccess;
         retire_batch(srv, s, ok);
         lock.lock();
       }
@@ -343,7 +395,7 @@ void scheduler_loop(clue_server* srv) {
       clue_status st = launch_batch(srv, free_slot, std::move(reqs));
       if (st != CLUE_OK) {
         free_slot->batch = std::move(keep);
-        cudaStreamSynchronize(free_slot->stream);
+        cudaStreamSynchronize(free_slot->active);
         retire_batch(srv, free_slot, false);
       }
       lock.lock();
@@ -356,6 +408,11 @@ void scheduler_loop(clue_server* srv) {
 void free_slot(Slot* s) {
   if (s->stream)
     cudaStreamSynchronize(s->stream);
+  if (s->stream_hi)
+    cudaStreamSynchronize(s->stream_hi);
+  for (cudaEvent_t ev : {s->ev_start, s->ev_end})
+    if (ev)
+      cudaEventDestroy(ev);
   if (s->ws)
     clue_workspace_destroy(s->ws);
   for (void* p : {(void*)s->d_coords, (void*)s->d_weight, (void*)s->d_cluster, (void*)s->d_seed,
@@ -368,6 +425,8 @@ void free_slot(Slot* s) {
       cudaFreeHost(p);
   if (s->stream)
     cudaStreamDestroy(s->stream);
+  if (s->stream_hi)
+    cudaStreamDestroy(s->stream_hi);
   delete s;
 }
 
@@ -381,6 +440,8 @@ clue_status clue_server_create(clue_server** out, const clue_server_config* cfg,
     return fail(CLUE_ERR_INVALID_ARGUMENT, "server config and at least one profile are required");
   if (cfg->max_inflight <= 0 || cfg->max_batch_events <= 0 || cfg->budget_bytes == 0)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "max_inflight, max_batch_events and budget must be positive");
+  if (!(cfg->max_batch_ms >= 0.0f) || !(cfg->priority_ms >= 0.0f))
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "max_batch_ms and priority_ms must be >= 0");
   int32_t max_dim = 1;
   for (int i = 0; i < n_profiles; ++i) {
     clue_status s = check_params(&profiles[i].params);
@@ -397,6 +458,7 @@ clue_status clue_server_create(clue_server** out, const clue_server_config* cfg,
   srv->cfg = *cfg;
   srv->profiles.assign(profiles, profiles + n_profiles);
   srv->queues.resize(n_profiles);
+  srv->ns_per_point.assign(n_profiles, 0.0);
   srv->max_dim = max_dim;
   // Device bytes per batch point: workspace scratch plus inputs and outputs.
   const int64_t per_slot = (int64_t)(cfg->budget_bytes / cfg->max_inflight);
@@ -423,7 +485,11 @@ clue_status clue_server_create(clue_server** out, const clue_server_config* cfg,
     s->server = srv;
     srv->slots.push_back(s);
     clue_status st = CLUE_OK;
-    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) ||
+    int prio_low = 0, prio_high = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)) ||
+        (e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, prio_low)) ||
+        (e = cudaStreamCreateWithPriority(&s->stream_hi, cudaStreamNonBlocking, prio_high)) ||
+        (e = cudaEventCreate(&s->ev_start)) || (e = cudaEventCreate(&s->ev_end)) ||
         (e = cudaMalloc(&s->d_coords, P * max_dim * sizeof(float))) ||
         (e = cudaMalloc(&s->d_weight, P * sizeof(float))) ||
         (e = cudaMalloc(&s->d_cluster, P * sizeof(int32_t))) ||
@@ -437,6 +503,7 @@ clue_status clue_server_create(clue_server** out, const clue_server_config* cfg,
         (e = cudaMallocHost(&s->h_rho, P * sizeof(float))) ||
         (e = cudaMallocHost(&s->h_nh, P * sizeof(int32_t))))
       st = fail_cuda(e, "server slot allocation");
+    s->active = s->stream;
     if (st == CLUE_OK)
       st = clue_workspace_create(&s->ws, cfg->device);
     if (st == CLUE_OK) {

@@ -303,6 +303,16 @@ typedef struct {
   int32_t max_batch_events; /* events per batch */
   int64_t max_batch_points; /* points per batch (0: derived from the budget) */
   int32_t linger_us;        /* how long a small batch may wait for company */
+  /* Target device time of one batch in ms (0: no time cap). The scheduler
+   * learns each profile's device time per point from finished batches (CUDA
+   * events) and stops adding events to a batch when its estimate reaches this;
+   * the first event always goes in. */
+  float max_batch_ms;
+  /* Batches whose estimated device time is at least this many ms (0: never)
+   * run on a high-priority stream, so the GPU schedules their blocks before
+   * those of concurrent batches and a large event does not stretch by sharing
+   * the GPU. */
+  float priority_ms;
 } clue_server_config;
 
 typedef struct {

@@ -60,11 +60,13 @@ def _host_points(ev, pinned=False):
     return p
 
 
-@pytest.mark.parametrize("pinned", [False, True])
-def test_results_are_the_same_alone_and_in_the_mix(pinned):
-    evs = _events(60, seed=1 if pinned else 2)
+@pytest.mark.parametrize("pinned,timed", [(False, False), (True, False), (True, True)])
+def test_results_are_the_same_alone_and_in_the_mix(pinned, timed):
+    # timed: batches capped by learned device time, long ones on the high-priority stream
+    evs = _events(60, seed=(1 if pinned else 2) + (10 if timed else 0))
+    extra = dict(max_batch_ms=0.3, priority_ms=0.2) if timed else {}
     with clue.Server([P2, P3], max_inflight=3, max_batch_events=16, budget_bytes=2 << 30,
-                     linger_us=500) as srv:
+                     linger_us=500, **extra) as srv:
         pts = [_host_points(ev, pinned) for _, ev in evs]
         tickets = [srv.submit(prof, p) for (prof, _), p in zip(evs, pts)]
         srv.drain()
@@ -132,3 +134,10 @@ def test_submit_rejects_what_the_server_cannot_take():
         p.set_tags(np.arange(ev.n))
         with pytest.raises(ValueError):
             srv.submit(0, p)
+
+
+def test_server_rejects_negative_time_targets():
+    with pytest.raises(ValueError):
+        clue.Server([P2], max_batch_ms=-1.0)
+    with pytest.raises(ValueError):
+        clue.Server([P2], priority_ms=float("nan"))
