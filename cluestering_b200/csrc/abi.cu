@@ -825,7 +825,9 @@ clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* param
       cudaEventRecord(ev[1], st);
       if (s == CLUE_OK && (s = wait_run(ws)) == CLUE_OK) {
         float x = 0.0f;
-        if ((e = cudaEventElapsedTime(&x, ev[0], ev[1])) != cudaSuccess)
+        // the run's own completion event precedes ev[1] on the stream
+        if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess ||
+            (e = cudaEventElapsedTime(&x, ev[0], ev[1])) != cudaSuccess)
           s = fail_cuda(e, "cudaEventElapsedTime");
         v.push_back(x);
       }

@@ -236,7 +236,7 @@ clue_status clue_make_clusters_batched_host(clue_workspace* ws, const clue_param
  *     receives the run's status word: 0, or nonzero when a bounded wait
  *     inside a kernel gave up. */
 #define CLUE_NOALLOC_MAX_POINTS 16384
-#define CLUE_NOALLOC_SCRATCH_BYTES (3u << 20)
+#define CLUE_NOALLOC_SCRATCH_BYTES (4u << 20)
 clue_status clue_make_clusters_device_noalloc(const clue_params* params, const clue_points* points,
                                               uint32_t* device_status, void* stream);
 

@@ -60,6 +60,41 @@ def test_noalloc_matches_the_workspace_path_on_two_calls_in_a_row():
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("ndim", [3, 10])
+def test_noalloc_takes_events_with_every_option_at_the_limit(ndim):
+    # the largest scratch the entry point carves: sigma, density uncertainty
+    # and tags on top of the coordinates, at the point limit (3-D adds the cell
+    # layout, 10-D the most coordinate planes)
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(74 + ndim)
+    if ndim == 3:
+        ev = W.layered_3d(MAX_POINTS, seed=74)
+        coords, weights, prm = ev.coords, ev.weights, (3.0, 10.0, 4.0)
+    else:
+        coords = rng.uniform(0.0, 4.0, (ndim, MAX_POINTS)).astype(np.float32)
+        weights = np.ones(MAX_POINTS, np.float32)
+        prm = (1.0, 2.0, 1.0)
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    sig = [rng.uniform(0.1, 0.5, MAX_POINTS).astype(np.float32) for _ in range(ndim)]
+    unc = rng.uniform(0.5, 1.5, MAX_POINTS).astype(np.float32)
+    tags = rng.permutation(MAX_POINTS).astype(np.int32)
+    mk = lambda: clue.PointsDevice(t(coords), t(weights), sigma=[t(x) for x in sig],
+                                   density_uncertainty=t(unc), tags=t(tags, torch.int32))
+    algo = clue.Clusterer(*prm)
+    ref = mk()
+    algo.make_clusters(ref)
+    got = mk()
+    stream = torch.cuda.Stream()
+    status = torch.full((1,), 123, dtype=torch.int32, device="cuda")
+    rc = _noalloc(algo, got, stream, status)
+    assert rc == L.OK, L.load().clue_last_error()
+    stream.synchronize()
+    assert int(status.item()) == 0
+    for a, b in zip(_outputs(got), _outputs(ref)):
+        assert np.array_equal(a, b)
+
+
 def test_noalloc_rejects_events_above_the_limit():
     torch = pytest.importorskip("torch")
     ev = W.single_2d(MAX_POINTS + 1, seed=73)
