@@ -196,6 +196,8 @@ size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
   CLUE_PLACE(cell_geom, float4, c.cells ? 2 * T : 0);
   CLUE_PLACE(cell_info, CellInfo, c.cells ? N : 0);
   CLUE_PLACE(cell_box, float4, c.cells ? 2 * N : 0);
+  CLUE_PLACE(rec_cell, float4, c.cells ? N : 0);
+  CLUE_PLACE(event_exact, int32_t, c.cells ? 4 * c.events : 0);
   CLUE_PLACE(seeds, int32_t, N);
   CLUE_PLACE(seed_event, int32_t, N);
   CLUE_PLACE(scan_desc, unsigned long long, c.scan_blocks);

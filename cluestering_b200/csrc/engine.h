@@ -47,6 +47,8 @@ struct DeviceBuffers {
   int32_t* cls_nh = nullptr;
   float4* rec_dens = nullptr;
   float4* rec_nh = nullptr;
+  float4* rec_cell = nullptr;      // density records in cell-layout order
+  int32_t* event_exact = nullptr;  // 4 per event: bounds for exact-sum density
   uint32_t* rec_tag = nullptr;
   // cell layout of the nearest-higher search (D = 2 or 3)
   int32_t* nh_pos = nullptr;

@@ -840,6 +840,10 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     a.cell_geom = b.cell_geom;
     a.cell_info = b.cell_info;
     a.cell_box = b.cell_box;
+    a.rec_cell = b.rec_cell;
+    a.event_exact = b.event_exact;
+    a.n_events = sh.n_events;
+    a.walk = b.cls_nh;  // k_work_order's scratch, free once it has run
   }
   CLUE_CHECK(launch_work_order(D, prm, a, st));
   CLUE_MARK(3);

@@ -25,6 +25,7 @@ namespace clue_impl {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr unsigned kFullMask = 0xffffffffu;
 // sqrtf(2.0f), correctly rounded (the reference's math::sqrt(TData{2})).
 constexpr float kSqrt2 = 1.41421356237309504880f;
 
@@ -362,26 +363,85 @@ __device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
   return __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
 }
 
+// Exponent of the lowest set bit of a positive finite float: x = m * 2^e with
+// m odd returns e.
+__device__ __forceinline__ int lsb_exponent(float x) {
+  const uint32_t bits = __float_as_uint(x);
+  const uint32_t ex = (bits >> 23) & 0xffu;
+  const uint32_t m = ex ? ((bits & 0x7fffffu) | 0x800000u) : (bits & 0x7fffffu);
+  return (ex ? (int)ex - 150 : -149) + (__ffs(m) - 1);
+}
+
+// Density records, in sorted order and (with the cell layout) in cell-layout
+// order. For the flat kernel also the per-event bounds of event_sums_exact:
+// the smallest lowest-bit exponent of any contribution (a neighbour's
+// fl(flat * w_j), the point's own w_i), the largest of each, and whether any
+// weight is negative, -0, NaN or infinite.
 template <int D>
 __global__ void __launch_bounds__(kThreads) k_pack_density(const RunParams p, const SweepArgs a) {
   if (blockIdx.x == 0 && threadIdx.x < 2)
     a.queue[threadIdx.x] = 0;  // the sweeps that follow start with no item taken
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
-       s += (int64_t)gridDim.x * blockDim.x) {
-    const float w = a.sw[s];
-    // flat: contribution of a neighbour is fl(flat * w_j) (ConvolutionalKernel.hpp:24-27)
-    const float v = p.kernel_kind == CLUE_KERNEL_FLAT ? __fmul_rn(p.kernel_p0, w) : w;
-    float4 r;
-    r.x = a.sx[s];
-    r.y = a.sx[a.n + s];
-    if (D == 2) {
-      r.z = v;
-      r.w = w;
-    } else {
-      r.z = a.sx[2 * a.n + s];
-      r.w = v;
+  const bool stats = p.kernel_kind == CLUE_KERNEL_FLAT && a.event_exact != nullptr;
+  const int lane = threadIdx.x & 31;
+  // every lane of a warp runs the same iterations (warp reductions below)
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < a.n; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = base + threadIdx.x;
+    const bool valid = s < a.n;
+    int e = -1, lsb = INT_MAX, bad = 0;
+    uint32_t vb = 0, wb = 0;
+    if (valid) {
+      const float w = a.sw[s];
+      // flat: contribution of a neighbour is fl(flat * w_j) (ConvolutionalKernel.hpp:24-27)
+      const float v = p.kernel_kind == CLUE_KERNEL_FLAT ? __fmul_rn(p.kernel_p0, w) : w;
+      float4 r;
+      r.x = a.sx[s];
+      r.y = a.sx[a.n + s];
+      if (D == 2) {
+        r.z = v;
+        r.w = w;
+      } else {
+        r.z = a.sx[2 * a.n + s];
+        r.w = v;
+      }
+      a.rec_dens[s] = r;
+      if (a.rec_cell)
+        a.rec_cell[a.nh_pos[s]] = r;
+      if (stats) {
+        e = a.sevt[s];
+        bad = !(w >= 0.0f) || signbit(w) || isinf(w) || isinf(v);
+        if (!bad) {
+          if (v > 0.0f)
+            lsb = min(lsb, lsb_exponent(v));
+          if (w > 0.0f)
+            lsb = min(lsb, lsb_exponent(w));
+          vb = __float_as_uint(v);
+          wb = __float_as_uint(w);
+        }
+      }
     }
-    a.rec_dens[s] = r;
+    if (!stats)
+      continue;
+    int32_t* st = a.event_exact;
+    const int e0 = __shfl_sync(kFullMask, e, 0);
+    if (__all_sync(kFullMask, !valid || e == e0)) {
+      lsb = __reduce_min_sync(kFullMask, lsb);
+      vb = __reduce_max_sync(kFullMask, vb);
+      wb = __reduce_max_sync(kFullMask, wb);
+      bad = __any_sync(kFullMask, bad);
+      if (lane == 0 && e0 >= 0) {
+        atomicMin(&st[4 * e0], lsb);
+        atomicMax(reinterpret_cast<unsigned*>(&st[4 * e0 + 1]), vb);
+        atomicMax(reinterpret_cast<unsigned*>(&st[4 * e0 + 2]), wb);
+        if (bad)
+          atomicOr(&st[4 * e0 + 3], 1);
+      }
+    } else if (valid) {
+      atomicMin(&st[4 * e], lsb);
+      atomicMax(reinterpret_cast<unsigned*>(&st[4 * e + 1]), vb);
+      atomicMax(reinterpret_cast<unsigned*>(&st[4 * e + 2]), wb);
+      if (bad)
+        atomicOr(&st[4 * e + 3], 1);
+    }
   }
 }
 
@@ -584,7 +644,6 @@ __device__ __forceinline__ void density_add_packed(const RunParams& p, unsigned 
 constexpr int kRing = 4;       // chunks of candidate records in flight per warp
 constexpr int kChunk = 32;     // records per chunk (kChunk / 32 per lane)
 constexpr int kMaxRows = 32;   // rows of a search box the streamed path handles
-constexpr unsigned kFullMask = 0xffffffffu;
 
 // Copies stream positions c * kChunk + lane + 32 k (row table off/qa, row
 // cursor rr) into ring slot c % kRing, then closes the lane's commit group for
@@ -656,6 +715,254 @@ __device__ __forceinline__ unsigned range_bits(int lo, int hi) {
   return (hi - lo == 32 ? 0xffffffffu : ((1u << (hi - lo)) - 1u)) << lo;
 }
 
+// ---------------------------------------------------------------------------
+// Exact-sum density (flat kernel).
+//
+// The reference adds a point's contributions in its tile order, and float
+// addition rounds, so in general only that order reproduces its bits. When
+// every contribution of an event (fl(flat * w_j) for a neighbour, w_i for the
+// point itself) is a non-negative integer multiple of u = 2^min_lsb and their
+// total over the event is at most 2^24 u, every partial sum of any subset is
+// an integer multiple of u no larger than 2^24 u, which binary32 represents
+// exactly: no addition rounds, and the ordered sum equals the exact sum in any
+// order (unit weights are the common case: multiples of 1/2). Such events skip
+// the ordered stream: a warp streams only the cells within reach of its 32
+// points, and each lane adds its in-range candidates from its own box's tiles,
+// the same candidate set as the reference's.
+// ---------------------------------------------------------------------------
+
+constexpr int kMaxSegs = 64;        // cell-row segments an exact-sum warp streams (2 per lane)
+constexpr int kMaxUnionTiles = 32;  // tiles of the warp's union box (one per lane)
+constexpr int kMaxStream = kMaxSegs > kMaxRows ? kMaxSegs : kMaxRows;
+
+// The bound is checked in double: the true bound n * max_v + max_w and 2^24 u
+// are multiples of u, so a true bound above 2^24 u is at least (2^24 + 1) u,
+// which the double product cannot round down to 2^24 u.
+__device__ __forceinline__ bool event_sums_exact(const SweepArgs& a, int e, int n_points) {
+  const int4 st = reinterpret_cast<const int4*>(a.event_exact)[e];
+  if (st.w != 0)
+    return false;
+  if (st.x == INT_MAX)
+    return true;  // every contribution is zero
+  const double bound = (double)n_points * (double)__int_as_float(st.y) + (double)__int_as_float(st.z);
+  return bound <= ldexp(1.0, 24 + st.x);
+}
+
+// One warp, exact-sum event. Returns false (nothing done) when the warp's
+// reach needs more than kMaxSegs segments or kMaxUnionTiles tiles; the caller
+// then takes the ordered stream. Warp-uniform: every lane calls it.
+template <int D>
+__device__ bool density_exact(const RunParams& p, const SweepArgs& a, const EventDesc& ev,
+                              const GridDesc& g, const float* xi, int s, float wi, const int* inf,
+                              const int* sup, bool ordered, const int* uinf, const int* usup,
+                              float4 (*ring)[kChunk], int* off, int* qa, int* seg, int4* tinfo,
+                              float& rho) {
+  const int lane = threadIdx.x & 31;
+  int nu[D];
+  int64_t n_union = 1;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    nu[d] = usup[d] - uinf[d] + 1;
+    n_union *= nu[d];
+  }
+  if (n_union > kMaxUnionTiles)
+    return false;
+  // bounding box of the warp's points, widened by the reach of dc: every
+  // candidate in range of a lane lies in a cell that meets it
+  const float R = reach(p.dc2);
+  float qlo[D], qhi[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    float lo = xi[d], hi = xi[d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(kFullMask, lo, o));
+      hi = fmaxf(hi, __shfl_xor_sync(kFullMask, hi, o));
+    }
+    qlo[d] = __fsub_rd(lo, R);
+    qhi[d] = __fadd_ru(hi, R);
+  }
+  // lane t < n_union: tile t of the union box (last dimension fastest) and
+  // its rows of cells within reach
+  int rows_t = 0, tb = 0, ts = 1;
+  int clo[D], chi[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    clo[d] = chi[d] = 0;
+  if (lane < n_union) {
+    int rem = lane, tile = ev.tile_base;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      tile += (uinf[d] + rem % nu[d]) * g.stride[d];
+      rem /= nu[d];
+    }
+    tb = a.tile_offset[tile];
+    if (a.tile_offset[tile + 1] > tb) {
+      ts = a.cell_s[tile];
+      float glo[D], ginv[D];
+      load_geom<D>(a, tile, glo, ginv);
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        clo[d] = cell_coord(qlo[d], glo[d], ginv[d], ts);
+        chi[d] = cell_coord(qhi[d], glo[d], ginv[d], ts);
+      }
+      rows_t = (chi[0] - clo[0] + 1) * (D == 3 ? chi[1] - clo[1] + 1 : 1);
+    }
+  }
+  int incl = rows_t;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFullMask, incl, o);
+    if (lane >= o)
+      incl += y;
+  }
+  const int K = __shfl_sync(kFullMask, incl, 31);
+  if (K > kMaxSegs)
+    return false;
+  const int first = incl - rows_t;
+  const int n1c = D == 3 ? chi[1] - clo[1] + 1 : 1;
+  if (lane < n_union) {
+    tinfo[lane] = make_int4(first, clo[0], D == 3 ? clo[1] : 0, n1c);
+    for (int r = 0; r < rows_t; ++r) {
+      const int c0 = clo[0] + r / n1c;
+      const int row_cell = D == 2 ? c0 * ts : (c0 * ts + clo[1] + r % n1c) * ts;
+      const int q0 = a.cell_info[tb + row_cell + clo[D - 1]].start;
+      off[first + r] = a.cell_info[tb + row_cell + chi[D - 1]].end - q0;  // length for now
+      qa[first + r] = q0;
+      seg[first + r] = lane;
+    }
+  }
+  __syncwarp();
+  // stream offsets of the segments
+  const int l0 = 2 * lane < K ? off[2 * lane] : 0;
+  const int l1 = 2 * lane + 1 < K ? off[2 * lane + 1] : 0;
+  int run = l0 + l1;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFullMask, run, o);
+    if (lane >= o)
+      run += y;
+  }
+  const int total = __shfl_sync(kFullMask, run, 31);
+  __syncwarp();
+  if (2 * lane < K)
+    off[2 * lane] = run - l0 - l1;
+  if (2 * lane + 1 < K)
+    off[2 * lane + 1] = run - l1;
+  if (lane == 0)
+    off[K] = total;
+  __syncwarp();
+  // tiles of the union box inside this lane's box, as a mask over union tiles
+  uint32_t tmask = 0;
+  if (ordered) {
+    if (D == 2) {
+      const uint32_t row = (uint32_t)((1ull << (sup[1] - inf[1] + 1)) - 1) << (inf[1] - uinf[1]);
+      for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
+        tmask |= row << ((b0 - uinf[0]) * nu[1]);
+    } else {
+      const uint32_t row = (uint32_t)((1ull << (sup[2] - inf[2] + 1)) - 1) << (inf[2] - uinf[2]);
+      for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
+        for (int b1 = inf[1]; b1 <= sup[1]; ++b1)
+          tmask |= row << (((b0 - uinf[0]) * nu[1] + (b1 - uinf[1])) * nu[2]);
+    }
+  }
+  const uint32_t all_tiles = (uint32_t)((1ull << n_union) - 1);
+  // stream position of the point itself: its cell's row segment in its tile
+  // (a point with a non-finite coordinate has nothing in range, itself
+  // included, and needs none)
+  int p_self = -1;
+  {
+    int own[D], t_own = 0;
+    bool in = ordered;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      own[d] = get_bin(g, p, xi[d], d);
+      in &= inf[d] <= own[d] && own[d] <= sup[d] && isfinite(xi[d]);
+      t_own = t_own * nu[d] + (own[d] - uinf[d]);
+    }
+    if (in) {
+      int tile = ev.tile_base;
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        tile += own[d] * g.stride[d];
+      const int4 ti = tinfo[t_own];
+      const int sq = a.cell_s[tile];
+      const int c = a.cell_slot[s] - a.tile_offset[tile];
+      const int c0 = D == 2 ? c / sq : c / (sq * sq);
+      const int c1 = D == 2 ? 0 : (c / sq) % sq;
+      const int k = ti.x + (c0 - ti.y) * ti.w + (D == 3 ? c1 - ti.z : 0);
+      if (k >= 0 && k < K)  // always, for a finite point inside its box
+        p_self = off[k] + (a.nh_pos[s] - qa[k]);
+    }
+  }
+  // cursor over this lane's accepted segments: [ilo, ihi) in stream positions
+  int kc = 0, ilo = INT_MAX, ihi = INT_MAX;
+  auto next_accepted = [&]() {
+    while (kc < K && !((tmask >> seg[kc]) & 1u))
+      ++kc;
+    if (kc < K) {
+      ilo = off[kc];
+      ihi = off[kc + 1];
+      ++kc;
+    } else {
+      ilo = ihi = INT_MAX;
+    }
+  };
+  const bool take_all = tmask == all_tiles;
+  if (!take_all)
+    next_accepted();
+  const int chunks = (total + kChunk - 1) / kChunk;
+  const unsigned long long xi_xy = pack2(xi[0], xi[1]);
+  const float4* __restrict__ rec = a.rec_cell;
+  int rr = 0;
+#pragma unroll
+  for (int c = 0; c < kRing - 1; ++c)
+    stream_issue(ring, off, qa, rec, c, lane, total, rr);
+  for (int c = 0; c < chunks; ++c) {
+    stream_issue(ring, off, qa, rec, c + kRing - 1, lane, total, rr);
+    cp_async_wait<kRing - 1>();
+    __syncwarp();
+    const ulonglong2* chunk = reinterpret_cast<const ulonglong2*>(ring[c % kRing]);
+    const int base = c * kChunk;
+    const int cnt = min(kChunk, total - base);
+    const int jself = p_self - base;
+    unsigned acc = 0xffffffffu;
+    if (!take_all) {
+      const int cend = base + cnt;
+      acc = 0;
+      while (ilo < cend) {
+        const int lo = max(ilo, base), hi = min(ihi, cend);
+        if (lo < hi)
+          acc |= range_bits(lo - base, hi - base);
+        if (ihi > cend)
+          break;
+        next_accepted();
+      }
+    }
+    // any order is exact here; the self record adds w_i, the others v_j
+    if (cnt == kChunk) {
+#pragma unroll 8
+      for (int j = 0; j < kChunk; ++j) {
+        float v;
+        const float d2 = packed_d2<D>(xi_xy, xi[2], chunk[j], v);
+        if (((acc >> j) & 1u) && d2 <= p.dc2)
+          rho = __fadd_rn(rho, j == jself ? wi : v);
+      }
+    } else {
+      for (int j = 0; j < cnt; ++j) {
+        float v;
+        const float d2 = packed_d2<D>(xi_xy, xi[2], chunk[j], v);
+        if (((acc >> j) & 1u) && d2 <= p.dc2)
+          rho = __fadd_rn(rho, j == jself ? wi : v);
+      }
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  return true;
+}
+
 // Local density, one point per lane. When the 32 lanes of a warp share one
 // search box (the work order groups each tile's points by box), the warp
 // streams the box's candidate records through a shared-memory ring of kRing
@@ -666,8 +973,10 @@ __device__ __forceinline__ unsigned range_bits(int lo, int hi) {
 template <int D, int KIND>
 __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p, const SweepArgs a) {
   __shared__ __align__(16) float4 s_ring[kThreads / 32][kRing][kChunk];
-  __shared__ int s_off[kThreads / 32][kMaxRows + 1];
-  __shared__ int s_qa[kThreads / 32][kMaxRows];
+  __shared__ int s_off[kThreads / 32][kMaxStream + 1];
+  __shared__ int s_qa[kThreads / 32][kMaxStream];
+  __shared__ int s_seg[kThreads / 32][kMaxSegs];
+  __shared__ int4 s_tinfo[kThreads / 32][kMaxUnionTiles];
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_dens;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -734,8 +1043,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
       hi = off[r] + (a.tile_offset[row + sup[D - 1] + 1] - qa[r]);
     };
     float rho = 0.0f;
-    bool streamed = false;  // warp-uniform
-    if (one_grid && rows64 >= 1 && rows64 <= kMaxRows) {
+    // events whose sums are exact in any order stream only the cells in reach
+    const bool exact = KIND == CLUE_KERNEL_FLAT && a.rec_cell != nullptr && one_grid && u_ordered &&
+                       __all_sync(kFullMask, event_sums_exact(a, a.sevt[s], ev.n));
+    bool done = false;  // warp-uniform: the exact-sum path handled the warp
+    if (exact)
+      done = density_exact<D>(p, a, ev, g, xi, s, wi, inf, sup, ordered, uinf, usup, ring, off, qa,
+                              s_seg[warp], s_tinfo[warp], rho);
+    bool streamed = false;  // warp-uniform: the ordered stream handles the warp
+    if (!done && one_grid && rows64 >= 1 && rows64 <= kMaxRows) {
       const int rows = (int)rows64;
       // row table: lane r holds row r of U
       int len = 0, start = 0;
@@ -859,7 +1175,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
       cp_async_wait<0>();
       __syncwarp();
     }
-    if (!streamed)
+    if (!streamed && !done)
       for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
         density_add<D, KIND>(p, xi, __ldg(&rec[q]), q == s, wi, rho);
       });
@@ -1045,13 +1361,38 @@ __device__ __forceinline__ void group_sync() {
     __syncthreads();
 }
 
+// Walk order of a tile's cells: strips of kStripRows rows of cells, each
+// strip column by column (3-D: z-slice by z-slice, each slice in strips), a
+// bijection onto 0 .. s^D - 1. Consecutive cells form compact patches (about
+// 4 x 4 cells for the 16 cells that hold 32 points on average).
+constexpr int kStripRows = 4;
+template <int D>
+__device__ __forceinline__ int strip_position(int c, int s) {
+  int c0, c1, z = 0;
+  if (D == 2) {
+    c0 = c / s;
+    c1 = c - c0 * s;
+  } else {
+    z = c % s;
+    const int c01 = c / s;
+    c0 = c01 / s;
+    c1 = c01 - c0 * s;
+  }
+  const int r0 = c0 - c0 % kStripRows;
+  const int rows = min(kStripRows, s - r0);
+  const int p2 = r0 * s + c1 * rows + (c0 - r0);
+  return D == 2 ? p2 : z * s * s + p2;
+}
+
 // Cell layout of tile t by a group of NT threads (one warp, or the whole block
 // for a large tile): cell of every point, the layout positions (a counting
-// sort by cell inside the tile's range), cell ranges and member boxes, and the
-// density sweep's work order for the tile. cnt holds the tile's s^D cell
-// counters, ccnt box_classes<D>() class counters.
+// sort by cell inside the tile's range), cell ranges and member boxes, the
+// walk order (strip_position) and the density sweep's work order for the
+// tile. cnt and cnt2 hold s^D cell counters each, ccnt box_classes<D>() class
+// counters.
 template <int D, int NT>
-__device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, int* cnt, int* ccnt) {
+__device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, int* cnt, int* ccnt,
+                           int* cnt2) {
   constexpr int E = box_classes<D>();
   const int tid = NT == 32 ? (threadIdx.x & 31) : (int)threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -1153,15 +1494,32 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
       a.cell_box[2 * (begin + c) + 1] = make_float4(mx[1], mx[D - 1], 0.0f, 0.0f);
     }
   }
-  // Density work order: the tile's points grouped by search-box class (the
-  // lanes of a warp share one box) and in cell-layout order inside a class
-  // (they are neighbours). A counting sort by class: rounds of 32 layout
-  // positions per warp, grouped within a round by __match_any_sync; one warp
-  // keeps the layout order inside a class, several warps interleave their
-  // rounds (any order inside a class is correct: it only decides which lane
-  // computes which point).
+  // Walk order: the layout positions with the cells taken in strip order,
+  // walk[begin + k] = layout position of the k-th point.
+  for (int c = tid; c < S; c += NT) {
+    const int c_end = c + 1 < S ? cnt[c] : m;  // cursors hold the cell ends
+    const int c_begin = c > 0 ? cnt[c - 1] : 0;
+    cnt2[strip_position<D>(c, s)] = c_end - c_begin;
+  }
+  group_sync<NT>();
+  if (tid < 32)
+    warp_scan_range(cnt2, S);
+  group_sync<NT>();
   for (int i = tid; i < m; i += NT) {
-    const int q = a.nh_q[begin + i];
+    const int c = a.cell_slot[a.nh_q[begin + i]] - begin;
+    const int c_begin = c > 0 ? cnt[c - 1] : 0;
+    a.walk[begin + cnt2[strip_position<D>(c, s)] + (i - c_begin)] = begin + i;
+  }
+  group_sync<NT>();
+  // Density work order: the tile's points grouped by search-box class (the
+  // lanes of a warp share one box) and in walk order inside a class (they are
+  // neighbours). A counting sort by class: rounds of 32 walk positions per
+  // warp, grouped within a round by __match_any_sync; one warp keeps the walk
+  // order inside a class, several warps interleave their rounds (any order
+  // inside a class is correct: it only decides which lane computes which
+  // point).
+  for (int i = tid; i < m; i += NT) {
+    const int q = a.nh_q[a.walk[begin + i]];
     float xq[D];
     const float zero[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -1188,7 +1546,7 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
       first = atomicAdd(&ccnt[c], __popc(grp));
     first = __shfl_sync(kFullMask, first, leader);
     if (valid)
-      a.work_dens[begin + first + __popc(grp & lane_mask_lt())] = a.nh_q[begin + i];
+      a.work_dens[begin + first + __popc(grp & lane_mask_lt())] = a.nh_q[a.walk[begin + i]];
   }
 }
 
@@ -1203,19 +1561,26 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
   constexpr int E = box_classes<D>();
   static_assert(kWarpCellSlots * kCellWarps <= kCellSlots, "warp counters fit the block's");
   __shared__ int s_cnt[kCellSlots];
+  __shared__ int s_cnt2[kCellSlots];
   __shared__ int s_cls[kCellWarps][E];
   const int warp = threadIdx.x >> 5;
+  // per-event bounds of the exact-sum test, filled by k_pack_density
+  if (a.event_exact)
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 4 * (int64_t)a.n_events;
+         i += (int64_t)gridDim.x * blockDim.x)
+      a.event_exact[i] = (i & 3) == 0 ? INT_MAX : 0;
   if ((int)blockIdx.x < warp_blocks) {
     const int64_t stride = (int64_t)warp_blocks * kCellWarps;
     for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
       if (a.tile_offset[t + 1] - a.tile_offset[t] > kLargeTilePoints)
         continue;
-      tile_cells<D, 32>(p, a, t, s_cnt + warp * kWarpCellSlots, s_cls[warp]);
+      tile_cells<D, 32>(p, a, t, s_cnt + warp * kWarpCellSlots, s_cls[warp],
+                        s_cnt2 + warp * kWarpCellSlots);
     }
   } else {
     const int n_large = *a.large_count;
     for (int k = (int)blockIdx.x - warp_blocks; k < n_large; k += (int)gridDim.x - warp_blocks)
-      tile_cells<D, kCellWarps * 32>(p, a, a.large_tiles[k], s_cnt, s_cls[0]);
+      tile_cells<D, kCellWarps * 32>(p, a, a.large_tiles[k], s_cnt, s_cls[0], s_cnt2);
   }
 }
 
@@ -1243,8 +1608,8 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
   }
 }
 
-// Nearest higher over the cell layout. Thread w takes layout position w, so a
-// warp holds neighbouring points. The own cell and its neighbours in the own
+// Nearest higher over the cell layout. Thread w takes the w-th point of the
+// walk order, so a warp holds neighbouring points. The own cell and its neighbours in the own
 // tile come first, which usually fixes a small delta; then every tile of the
 // reference's search box is visited, but only its cells that can hold a point
 // within the current bound. The result is the eligible candidate of least
@@ -1269,7 +1634,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunP
     const int64_t w = item * 32 + lane;
     if (w >= n)
       continue;
-    const int pi = (int)w;
+    const int pi = a.walk[w];  // neighbouring points in neighbouring lanes
     const int s = a.nh_q[pi];
     const float4 ri = rec[pi];
     const float xi[3] = {ri.x, ri.y, ri.z};

@@ -35,6 +35,19 @@ struct SweepArgs {
   // k_cells gives each of them a whole block.
   const int32_t* large_tiles;
   const int32_t* large_count;
+  // Exact-sum density (flat kernel): the density records again, in cell-layout
+  // order, and per event four bounds on its contributions (smallest lowest-set-
+  // bit exponent, largest neighbour contribution and largest weight as float
+  // bits, and a flag for a negative or non-finite one) that decide whether the
+  // event's sums are exact in any order. Null when the cell layout is off.
+  float4* rec_cell;
+  int32_t* event_exact;
+  int32_t n_events;
+  // Walk order of the cell layout (k_cells): walk[k] is the layout position
+  // visited k-th, tile by tile, cells in strips of 4 rows so that consecutive
+  // points are spatial neighbours. Orders the density work and the
+  // nearest-higher threads.
+  int32_t* walk;
   // Packed candidate records of the fast path (D = 2 or 3).
   float4* rec_dens;  // {x, y, [z], v}: v = flat * w for the flat kernel, else w
   float4* rec_nh;    // D = 2: {x, y, rho, tag bits}; D = 3: {x, y, z, rho}
