@@ -925,7 +925,6 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
     const ulonglong2* chunk = reinterpret_cast<const ulonglong2*>(ring[c % kRing]);
     const int base = c * kChunk;
     const int cnt = min(kChunk, total - base);
-    const int jself = p_self - base;
     unsigned acc = 0xffffffffu;
     if (!take_all) {
       const int cend = base + cnt;
@@ -939,27 +938,33 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
         next_accepted();
       }
     }
-    // any order is exact here; the self record adds w_i, the others v_j
-    if (cnt == kChunk) {
+    // Any order is exact here. Every record in range adds its v_j, the
+    // point's own record included; the own term is corrected once at the end.
+    if (cnt == kChunk && __all_sync(kFullMask, acc == 0xffffffffu)) {
 #pragma unroll 8
       for (int j = 0; j < kChunk; ++j) {
         float v;
         const float d2 = packed_d2<D>(xi_xy, xi[2], chunk[j], v);
-        if (((acc >> j) & 1u) && d2 <= p.dc2)
-          rho = __fadd_rn(rho, j == jself ? wi : v);
+        if (d2 <= p.dc2)
+          rho = __fadd_rn(rho, v);
       }
     } else {
       for (int j = 0; j < cnt; ++j) {
         float v;
         const float d2 = packed_d2<D>(xi_xy, xi[2], chunk[j], v);
         if (((acc >> j) & 1u) && d2 <= p.dc2)
-          rho = __fadd_rn(rho, j == jself ? wi : v);
+          rho = __fadd_rn(rho, v);
       }
     }
     __syncwarp();
   }
   cp_async_wait<0>();
   __syncwarp();
+  // The own record (d2 = 0, in range) added v_i = fl(flat * w_i) where the
+  // reference adds w_i: (rho - v_i) + w_i, both steps exact (multiples of u,
+  // between 0 and the event bound).
+  if (p_self >= 0)
+    rho = __fadd_rn(__fsub_rn(rho, __fmul_rn(p.kernel_p0, wi)), wi);
   return true;
 }
 
