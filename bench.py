@@ -49,9 +49,9 @@ CONFIG = {
 BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4 * D + 12,
                    "pipeline": lambda D: 20 * D + 64}
 # DRAM bytes (read + write) per point of each sweep, from one ncu capture of the
-# 1,024-event batch (profiles/sweeps_batch_2d_1024ev.md: 893.8 MB and 644.2 MB
+# 1,024-event batch (profiles/sweeps_batch_2d_1024ev.md: 922.5 MB and 651.8 MB
 # for 10,621,973 points); a launch's traffic grows with the points it processes.
-DRAM_BYTES_PER_POINT = {"density": 84.1, "nearest_higher": 60.6}
+DRAM_BYTES_PER_POINT = {"density": 86.9, "nearest_higher": 61.4}
 
 
 def measured_peaks():
@@ -280,9 +280,11 @@ def run_ours(args, world, rank, local):
                      "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": DRAM_BYTES_PER_POINT[dom] * n_total,
                      "peak_kind": peak_kind,
-                     "note": "sweeps are issue/latency bound: each point tests ~855 candidates "
-                             "in the reference's tile order; achieved counts algorithmic bytes, "
-                             "traffic is ncu DRAM bytes per point scaled to this launch"},
+                     "note": "the sweeps are instruction-issue bound, not HBM bound: each point "
+                             "tests hundreds of candidate records (density: ~820 per warp, read "
+                             "from shared memory, 85% issue active in ncu); achieved counts "
+                             "algorithmic bytes, traffic is ncu DRAM bytes per point scaled to "
+                             "this launch"},
         "clocks": clocks.summary(),
         "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": os.cpu_count() or 1,
                          "kind": "port", "sample": cpu_sample},
