@@ -20,7 +20,11 @@ from .api import (  # noqa: F401
     Server,
     WeightedChebyshevMetric,
     WeightedEuclideanMetric,
+    cluster_centroids,
     clusters_csr,
     metrics,
+    silhouette,
+    silhouette_scores,
+    weighted_cluster_centroids,
 )
 from ._lib import GRID_PER_EVENT, GRID_SHARED, ClueError  # noqa: F401

@@ -126,6 +126,8 @@ SIGNATURES = {
     "clue_get_seeds": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "clue_get_clusters_device": (C.c_int, [_P, _P, _P, _P]),
     "clue_sample_associations": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
+    "clue_cluster_centroids_device": (C.c_int, [C.POINTER(Points), _P, _P, C.c_int32, C.c_int32, _P, _P]),
+    "clue_silhouette_device": (C.c_int, [C.POINTER(Points), _P, _P, C.c_int32, _P, _P]),
     "clue_stream_create": (C.c_int, [C.POINTER(_P), C.c_int32]),
     "clue_stream_destroy": (C.c_int, [_P]),
     "clue_stream_synchronize": (C.c_int, [_P]),

@@ -473,6 +473,63 @@ class Clusterer:
 
 
 # ---------------------------------------------------------------------------
+# Validation utilities on the device (utils/cluster_centroid.hpp, utils/scores.hpp)
+# ---------------------------------------------------------------------------
+
+
+def _device_map(points, clusterer, stream):
+    if not isinstance(points, PointsDevice):
+        raise TypeError("the device utilities take the PointsDevice the clusterer last clustered")
+    if not getattr(points, "clustered", False):
+        raise RuntimeError("the points have not been clustered")
+    offsets, members = clusterer.getClustersDevice(stream)
+    return offsets, members, len(offsets) - 1
+
+
+def cluster_centroids(points, clusterer, *, weighted: bool = False, stream=None) -> np.ndarray:
+    """clue::cluster_centroids / weighted_cluster_centroids
+    (utils/detail/cluster_centroid.hpp:86-140) of `clusterer`'s last run on
+    `points`, computed on the device: (n_clusters, ndim) float32, the reference's
+    values bit for bit."""
+    import torch
+    offsets, members, k = _device_map(points, clusterer, stream)
+    out = torch.zeros((max(k, 1), points.ndim), dtype=torch.float32, device=points.coords.device)
+    st = Clusterer._stream_handle(stream, False)
+    L.check(L.load().clue_cluster_centroids_device(C.byref(_points_struct(points)), offsets.data_ptr(),
+                                                   members.data_ptr(), k, int(weighted), out.data_ptr(), st))
+    L.check(L.load().clue_stream_synchronize(st))
+    return out[:k].cpu().numpy()
+
+
+def weighted_cluster_centroids(points, clusterer, *, stream=None) -> np.ndarray:
+    return cluster_centroids(points, clusterer, weighted=True, stream=stream)
+
+
+def silhouette_scores(points, clusterer, *, stream=None) -> np.ndarray:
+    """clue::silhouette(points, point) for every point (utils/detail/scores.hpp:33-73),
+    on the device; NaN for the points the reference's mean skips."""
+    import torch
+    offsets, members, k = _device_map(points, clusterer, stream)
+    scores = torch.empty(points.size(), dtype=torch.float32, device=points.coords.device)
+    st = Clusterer._stream_handle(stream, False)
+    L.check(L.load().clue_silhouette_device(C.byref(_points_struct(points)), offsets.data_ptr(),
+                                            members.data_ptr(), k, scores.data_ptr(), st))
+    L.check(L.load().clue_stream_synchronize(st))
+    return scores.cpu().numpy()
+
+
+def silhouette(points, clusterer, point: int | None = None, *, stream=None) -> float:
+    """clue::silhouette(points) (the mean over the points of clusters with at
+    least two points, utils/detail/scores.hpp:76-100) or, with `point`,
+    clue::silhouette(points, point)."""
+    s = silhouette_scores(points, clusterer, stream=stream)
+    if point is not None:
+        return float(s[point])
+    keep = s[~np.isnan(s)]
+    return float(np.mean(keep.astype(np.float64))) if keep.size else float("nan")
+
+
+# ---------------------------------------------------------------------------
 # Serving (continuous batching; no counterpart in the reference)
 # ---------------------------------------------------------------------------
 

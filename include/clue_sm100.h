@@ -259,6 +259,33 @@ clue_status clue_get_seeds(clue_workspace* ws, int32_t* seeds, int32_t capacity,
 clue_status clue_get_clusters_device(clue_workspace* ws, int32_t* offsets, int32_t* points,
                                      void* stream);
 
+/* ---- validation utilities -------------------------------------------------- */
+/* Both take a cluster map as clue_get_clusters_device writes it (offsets with
+ * n_clusters + 1 entries, point ids ascending within a cluster), the points'
+ * device buffers, and allocate nothing; asynchronous on stream.
+ *
+ * clue::cluster_centroids / weighted_cluster_centroids
+ * (utils/detail/cluster_centroid.hpp:86-140): centroids[c * ndim + d] is the
+ * float sum of coordinate d (weighted: of coordinate * weight) over cluster c's
+ * points in ascending index order, divided by the cluster's size (weighted: by
+ * the sum of its weights in the same order) — the reference's values bit for
+ * bit. points->weight is needed when weighted. */
+clue_status clue_cluster_centroids_device(const clue_points* points, const int32_t* cluster_offsets,
+                                          const int32_t* cluster_points, int32_t n_clusters,
+                                          int32_t weighted, float* centroids, void* stream);
+/* clue::silhouette(points, point) for every point (utils/detail/scores.hpp:33-73):
+ * scores[i] = (b - a) / max(a, b) with a the mean distance from i to the other
+ * points of its cluster and b the smallest mean distance to another cluster
+ * (FLT_MAX when there is none), Euclidean distances, sums in cluster order —
+ * the reference's per-point values bit for bit; NaN for points the reference's
+ * mean skips (label -1 or a cluster of one point). Reads
+ * points->cluster_index as the labels. Work grows as n times the clustered
+ * points, like the reference's. clue::silhouette(points) is the mean of the
+ * non-NaN scores. */
+clue_status clue_silhouette_device(const clue_points* points, const int32_t* cluster_offsets,
+                                   const int32_t* cluster_points, int32_t n_clusters, float* scores,
+                                   void* stream);
+
 /* Clusterer::getSampleAssociations (core/detail/Clusterer.hpp:219-242): event
  * -> cluster ids of the last batched run, as CSR in host memory. offsets has
  * n_events + 1 entries; cluster ids of event e are offsets[e]..offsets[e+1]-1

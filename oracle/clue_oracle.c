@@ -533,3 +533,87 @@ int clue_oracle_make_clusters_batched(const oracle_params* prm, const oracle_poi
   }
   return 0;
 }
+
+/* ---- validation utilities (utils/detail/cluster_centroid.hpp, scores.hpp) ---- */
+
+/* Cluster -> points in ascending index order (utils/detail/get_clusters.hpp:24-49):
+ * offsets[n_clusters + 1], members[offsets[n_clusters]]. */
+static void cluster_map(int32_t n, const int32_t* labels, int32_t n_clusters, int32_t* offsets,
+                        int32_t* members) {
+  memset(offsets, 0, sizeof(int32_t) * (size_t)(n_clusters + 1));
+  for (int32_t i = 0; i < n; ++i)
+    if (labels[i] >= 0 && labels[i] < n_clusters)
+      ++offsets[labels[i] + 1];
+  for (int32_t c = 0; c < n_clusters; ++c)
+    offsets[c + 1] += offsets[c];
+  int32_t* cursor = malloc(sizeof(int32_t) * (size_t)(n_clusters + 1));
+  memcpy(cursor, offsets, sizeof(int32_t) * (size_t)(n_clusters + 1));
+  for (int32_t i = 0; i < n; ++i)
+    if (labels[i] >= 0 && labels[i] < n_clusters)
+      members[cursor[labels[i]]++] = i;
+  free(cursor);
+}
+
+void clue_oracle_centroids(int32_t ndim, int32_t n, const float* const* coords, const float* weights,
+                           const int32_t* labels, int32_t n_clusters, int32_t weighted, float* out) {
+  int32_t* offsets = malloc(sizeof(int32_t) * (size_t)(n_clusters + 1));
+  int32_t* members = malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  cluster_map(n, labels, n_clusters, offsets, members);
+  for (int32_t c = 0; c < n_clusters; ++c) {
+    for (int32_t d = 0; d < ndim; ++d) {
+      float sum = 0.0f, total = 0.0f;
+      for (int32_t k = offsets[c]; k < offsets[c + 1]; ++k) {
+        const int32_t i = members[k];
+        sum += weighted ? coords[d][i] * weights[i] : coords[d][i];
+        total += weights ? weights[i] : 0.0f;
+      }
+      const int32_t size = offsets[c + 1] - offsets[c];
+      out[(size_t)c * ndim + d] = weighted ? sum / total : sum / (float)size;
+    }
+  }
+  free(offsets);
+  free(members);
+}
+
+/* utils/detail/scores.hpp:24-31: sqrt of the left fold of squared differences. */
+static float silhouette_distance(int32_t ndim, const float* const* x, int32_t i, int32_t j) {
+  float dist = 0.0f;
+  for (int32_t d = 0; d < ndim; ++d) {
+    const float diff = x[d][i] - x[d][j];
+    dist += diff * diff;
+  }
+  return sqrtf(dist);
+}
+
+void clue_oracle_silhouette(int32_t ndim, int32_t n, const float* const* coords, const int32_t* labels,
+                            int32_t n_clusters, float* scores) {
+  int32_t* offsets = malloc(sizeof(int32_t) * (size_t)(n_clusters + 1));
+  int32_t* members = malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  cluster_map(n, labels, n_clusters, offsets, members);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int32_t i = 0; i < n; ++i) {
+    const int32_t own = labels[i];
+    if (own < 0 || own >= n_clusters || offsets[own + 1] - offsets[own] < 2) {
+      scores[i] = NAN;
+      continue;
+    }
+    float a = 0.0f, b = FLT_MAX;
+    for (int32_t c = 0; c < n_clusters; ++c) {
+      float sum = 0.0f;
+      for (int32_t k = offsets[c]; k < offsets[c + 1]; ++k)
+        if (members[k] != i)
+          sum += silhouette_distance(ndim, coords, i, members[k]);
+      const int32_t count = offsets[c + 1] - offsets[c];
+      if (c == own) {
+        a = sum / (float)(count - 1);
+      } else {
+        const float mean = sum / (float)count;
+        b = mean < b ? mean : b;  /* std::min(acc, val) */
+      }
+    }
+    const float hi = a < b ? b : a;  /* std::max(a, b) */
+    scores[i] = (b - a) / hi;
+  }
+  free(offsets);
+  free(members);
+}

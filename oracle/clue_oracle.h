@@ -96,6 +96,22 @@ int clue_oracle_make_clusters_batched(const oracle_params* params, const oracle_
 /* The library-owned exponential, exposed so tests can check its error. */
 float clue_oracle_expf(float x);
 
+/* Cluster centroids (utils/detail/cluster_centroid.hpp:86-140): for every
+ * cluster c < n_clusters and dimension d, the float sum of coords[d][i] (or of
+ * coords[d][i] * weights[i] when weighted) over the points with label c in
+ * ascending index order, divided by the cluster's size (or by the float sum of
+ * its weights, accumulated in the same order). out is n_clusters x ndim. */
+void clue_oracle_centroids(int32_t ndim, int32_t n, const float* const* coords, const float* weights,
+                           const int32_t* labels, int32_t n_clusters, int32_t weighted, float* out);
+
+/* Silhouette of every point (utils/detail/scores.hpp:33-73): the points of
+ * every cluster in ascending index order, distance sqrt of the left fold of
+ * squared differences, a = own-cluster mean without the point itself, b = the
+ * smallest other-cluster mean (FLT_MAX when there is none), (b - a) / max(a, b).
+ * Points with label -1 or in a cluster of one point get NaN. */
+void clue_oracle_silhouette(int32_t ndim, int32_t n, const float* const* coords, const int32_t* labels,
+                            int32_t n_clusters, float* scores);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,6 +106,12 @@ def _load():
         lib.clue_oracle_make_clusters_batched.restype = C.c_int
         lib.clue_oracle_expf.argtypes = [C.c_float]
         lib.clue_oracle_expf.restype = C.c_float
+        lib.clue_oracle_centroids.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_int32, C.c_int32, C.c_void_p]
+        lib.clue_oracle_centroids.restype = None
+        lib.clue_oracle_silhouette.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                               C.c_void_p]
+        lib.clue_oracle_silhouette.restype = None
         _lib = lib
     return _lib
 
@@ -243,3 +249,32 @@ def make_clusters_batched(coords, weights, event_sizes, dc, rhoc, dm=None, seed_
 
 def expf(x: float) -> float:
     return float(_load().clue_oracle_expf(float(x)))
+
+
+def _coord_table(coords):
+    coords = np.ascontiguousarray(coords, dtype=np.float32)
+    if coords.ndim == 1:
+        coords = coords[None, :]
+    table = (C.c_void_p * coords.shape[0])(*[coords[d].ctypes.data for d in range(coords.shape[0])])
+    return coords, table
+
+
+def centroids(coords, weights, labels, n_clusters: int, weighted: bool = False) -> np.ndarray:
+    """utils/detail/cluster_centroid.hpp:86-140: (n_clusters, D) float32 centroids."""
+    coords, table = _coord_table(coords)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    out = np.zeros((max(n_clusters, 0), coords.shape[0]), np.float32)
+    _load().clue_oracle_centroids(coords.shape[0], coords.shape[1], table, w.ctypes.data, lab.ctypes.data,
+                                  n_clusters, int(weighted), out.ctypes.data)
+    return out
+
+
+def silhouette(coords, labels, n_clusters: int) -> np.ndarray:
+    """utils/detail/scores.hpp:33-73 for every point (NaN where the reference skips it)."""
+    coords, table = _coord_table(coords)
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    out = np.zeros(coords.shape[1], np.float32)
+    _load().clue_oracle_silhouette(coords.shape[0], coords.shape[1], table, lab.ctypes.data, n_clusters,
+                                   out.ctypes.data)
+    return out
