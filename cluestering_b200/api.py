@@ -412,6 +412,16 @@ class Clusterer:
         L.check(L.load().clue_stream_synchronize(st))
         return offsets, pts[: int(offsets[-1].item())]
 
+    def set_graphs(self, enable: bool = True) -> None:
+        """CUDA-graph replay of repeated identical runs (clue_workspace_set_graphs)."""
+        L.check(L.load().clue_workspace_set_graphs(self._workspace(), int(enable)))
+
+    def graph_replayed(self) -> bool:
+        """Whether the last run replayed a captured graph."""
+        r = C.c_int32()
+        L.check(L.load().clue_workspace_graph_replayed(self._workspace(), C.byref(r)))
+        return bool(r.value)
+
     def set_profiling(self, enable: bool = True) -> None:
         L.check(L.load().clue_workspace_set_profiling(self._workspace(), int(enable)))
 

@@ -429,14 +429,18 @@ RunParams make_run_params(const clue_params* p, const clue_points* pts, const cl
 }
 
 // Uploads the host tables through the workspace's pinned staging buffer.
-clue_status upload_tables(clue_workspace* ws, const HostTables& t, cudaStream_t st) {
+// Copies the run tables into the pinned staging buffer, after the previous
+// upload has left it (a host wait: done before any stream capture).
+clue_status stage_tables(clue_workspace* ws, const HostTables& t) {
   const size_t g = t.grids.size() * sizeof(GridDesc);
   const size_t e = t.events.size() * sizeof(EventDesc);
   const size_t c = t.chunks.size() * sizeof(Chunk);
   const size_t need = g + e + c;
-  // The previous upload must have left the staging buffer before it is reused.
-  if (ws->staging_event)
-    cudaEventSynchronize(ws->staging_event);
+  if (ws->staging_event) {
+    const cudaError_t err = cudaEventSynchronize(ws->staging_event);
+    if (err != cudaSuccess)
+      return fail_cuda(err, "table staging wait");
+  }
   if (ws->staging_bytes < need) {
     if (ws->staging)
       cudaFreeHost(ws->staging);
@@ -451,16 +455,81 @@ clue_status upload_tables(clue_workspace* ws, const HostTables& t, cudaStream_t 
   std::memcpy(h, t.grids.data(), g);
   std::memcpy(h + g, t.events.data(), e);
   std::memcpy(h + g + e, t.chunks.data(), c);
+  return CLUE_OK;
+}
+
+// Stream part of the table upload. `record` marks the staging buffer free
+// again once the copies are done; a captured run records that mark after its
+// graph launch instead (an event recorded inside a capture cannot be waited on
+// from the host).
+clue_status copy_tables(clue_workspace* ws, const HostTables& t, cudaStream_t st, bool record) {
+  const size_t g = t.grids.size() * sizeof(GridDesc);
+  const size_t e = t.events.size() * sizeof(EventDesc);
+  const size_t c = t.chunks.size() * sizeof(Chunk);
+  const char* h = (const char*)ws->staging;
   cudaError_t err;
   if ((err = cudaMemcpyAsync(ws->b.grids, h, g, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (err = cudaMemcpyAsync(ws->b.events, h + g, e, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (err = cudaMemcpyAsync(ws->b.chunks, h + g + e, c, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return fail_cuda(err, "table upload");
-  cudaEventRecord(ws->staging_event, st);
+  if (record && (err = cudaEventRecord(ws->staging_event, st)) != cudaSuccess)
+    return fail_cuda(err, "table upload event");
   return CLUE_OK;
 }
 
-// One run on device-resident points. `sizes` is the host event table.
+namespace {
+
+bool same_bits(float a, float b) {
+  uint32_t x, y;
+  std::memcpy(&x, &a, 4);
+  std::memcpy(&y, &b, 4);
+  return x == y;
+}
+
+bool same_params(const clue_params& a, const clue_params& b) {
+  bool same = same_bits(a.dc, b.dc) && same_bits(a.rhoc, b.rhoc) && same_bits(a.dm, b.dm) &&
+              same_bits(a.seed_dc, b.seed_dc) && a.kernel_kind == b.kernel_kind &&
+              same_bits(a.kernel_params[0], b.kernel_params[0]) &&
+              same_bits(a.kernel_params[1], b.kernel_params[1]) && a.metric_kind == b.metric_kind &&
+              a.points_per_tile == b.points_per_tile;
+  for (int d = 0; d < CLUE_MAX_DIM; ++d)
+    same = same && a.wrapped[d] == b.wrapped[d] && same_bits(a.metric_params[d], b.metric_params[d]);
+  return same;
+}
+
+bool same_points(const clue_points& a, const clue_points& b) {
+  bool same = a.ndim == b.ndim && a.n == b.n && a.weight == b.weight &&
+              a.density_uncertainty == b.density_uncertainty && a.tags == b.tags &&
+              a.cluster_index == b.cluster_index && a.is_seed == b.is_seed && a.rho == b.rho &&
+              a.nearest_higher == b.nearest_higher;
+  for (int d = 0; same && d < a.ndim; ++d)
+    same = a.coords[d] == b.coords[d] && a.sigma[d] == b.sigma[d];
+  return same;
+}
+
+// Whether a run with these arguments is the one the cached graph was captured for.
+bool graph_matches(const clue_workspace* ws, const clue_params* params, const clue_points* pts,
+                   const uint32_t* sizes, int32_t n_events, int32_t grid_mode, int64_t staged) {
+  const auto& k = ws->graph_key;
+  if (!ws->graph_exec || k.grid_mode != grid_mode || k.staged != staged || k.base != ws->base ||
+      (int64_t)k.sizes.size() != n_events || !same_params(k.params, *params) ||
+      !same_points(k.points, *pts) ||
+      std::memcmp(&k.tuning, &ws->tuning, sizeof(clue_tuning)) != 0)
+    return false;
+  return std::memcmp(k.sizes.data(), sizes, sizeof(uint32_t) * (size_t)n_events) == 0;
+}
+
+}  // namespace
+
+clue_status upload_tables(clue_workspace* ws, const HostTables& t, cudaStream_t st) {
+  clue_status s = stage_tables(ws, t);
+  return s != CLUE_OK ? s : copy_tables(ws, t, st, true);
+}
+
+// One run on device-resident points. `sizes` is the host event table. With
+// graphs on (and a non-default stream, no stage timing), the run is captured
+// into a CUDA graph, and a later run with identical arguments replays it: no
+// table building, no per-kernel launches, one graph launch.
 clue_status run_device(clue_workspace* ws, const clue_params* params, const clue_points* pts,
                        const uint32_t* sizes, int32_t n_events, int32_t grid_mode,
                        cudaStream_t st, int64_t staged) {
@@ -472,6 +541,17 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   cudaError_t e = cudaSetDevice(ws->device);
   if (e != cudaSuccess)
     return fail_cuda(e, "cudaSetDevice");
+  const bool use_graph = ws->graphs && !ws->profiling && st != nullptr;
+  if (use_graph && graph_matches(ws, params, pts, sizes, n_events, grid_mode, staged)) {
+    if ((e = cudaGraphLaunch(ws->graph_exec, st)) != cudaSuccess ||
+        (e = cudaEventRecord(ws->staging_event, st)) != cudaSuccess)
+      return fail_cuda(e, "graph launch");
+    cudaEventRecord(ws->run_event, st);
+    ws->has_run = true;
+    ws->graph_replays_last = true;
+    return CLUE_OK;
+  }
+  ws->graph_replays_last = false;
   HostTables t;
   RunShape sh;
   const char* err = nullptr;
@@ -485,8 +565,17 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   if ((s = ensure_capacity(ws, sh, any_sigma, pts->density_uncertainty != nullptr,
                            pts->tags != nullptr, staged)) != CLUE_OK)
     return s;
-  if ((s = upload_tables(ws, t, st)) != CLUE_OK)
+  if ((s = stage_tables(ws, t)) != CLUE_OK)
     return s;
+  if (ws->graph_exec) {  // the cached graph reads the staging buffer just overwritten
+    if ((e = cudaGraphExecDestroy(ws->graph_exec)) != cudaSuccess)
+      return fail_cuda(e, "graph release");
+    ws->graph_exec = nullptr;
+  }
+  // a failure of an earlier call whose status was not read would show up as
+  // this run's launch error
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return fail_cuda(e, "a CUDA error left pending before this run");
   RunIO io;
   for (int d = 0; d < pts->ndim; ++d) {
     io.coords[d] = pts->coords[d];
@@ -501,13 +590,48 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   io.nh = pts->nearest_higher;
   const RunParams prm = make_run_params(params, pts, ws->tuning);
   reset_launch_count();
-  if ((e = launch_run(sh, prm, io, ws->b, st, ws->profiling ? ws->marks : nullptr)) != cudaSuccess)
-    return fail_cuda(e, "kernel launch");
-  ws->last_launches = launch_count();
+  if (use_graph && (e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return fail_cuda(e, "stream capture");
+  // Everything from here to the end of the capture is stream work.
+  s = copy_tables(ws, t, st, !use_graph);
+  if (s == CLUE_OK && (e = launch_run(sh, prm, io, ws->b, st, ws->profiling ? ws->marks : nullptr)) !=
+                          cudaSuccess)
+    s = fail_cuda(e, "kernel launch");
   // Seed count and status word come back with the run (read when needed).
-  cudaMemcpyAsync(&ws->info->n_seeds, ws->b.counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                  st);
-  cudaMemcpyAsync(&ws->info->status, ws->b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  if (s == CLUE_OK &&
+      ((e = cudaMemcpyAsync(&ws->info->n_seeds, ws->b.counters + 1, sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+       (e = cudaMemcpyAsync(&ws->info->status, ws->b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            st)) != cudaSuccess))
+    s = fail_cuda(e, "result copy");
+  if (use_graph) {
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+    if (s == CLUE_OK && ec != cudaSuccess)
+      s = fail_cuda(ec, "stream capture");
+    if (s == CLUE_OK && (e = cudaGraphInstantiate(&ws->graph_exec, graph, 0)) != cudaSuccess) {
+      ws->graph_exec = nullptr;
+      s = fail_cuda(e, "graph instantiation");
+    }
+    if (graph)
+      cudaGraphDestroy(graph);
+    if (s == CLUE_OK && ((e = cudaGraphLaunch(ws->graph_exec, st)) != cudaSuccess ||
+                         (e = cudaEventRecord(ws->staging_event, st)) != cudaSuccess))
+      s = fail_cuda(e, "graph launch");
+    if (s == CLUE_OK) {
+      auto& k = ws->graph_key;
+      k.params = *params;
+      k.points = *pts;
+      k.tuning = ws->tuning;
+      k.grid_mode = grid_mode;
+      k.staged = staged;
+      k.base = ws->base;
+      k.sizes.assign(sizes, sizes + n_events);
+    }
+  }
+  if (s != CLUE_OK)
+    return s;
+  ws->last_launches = launch_count();
   cudaEventRecord(ws->run_event, st);
   ws->has_run = true;
   ws->last_n = sh.n;
@@ -694,6 +818,8 @@ clue_status clue_workspace_destroy(clue_workspace* ws) {
   for (auto& m : ws->marks)
     if (m)
       cudaEventDestroy(m);
+  if (ws->graph_exec)
+    cudaGraphExecDestroy(ws->graph_exec);
   delete ws;
   return CLUE_OK;
 }
@@ -720,6 +846,27 @@ clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tun
   if (tuning->label_jump_rounds < -1 || tuning->label_jump_rounds > 4)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "label_jump_rounds must be in [-1, 4]");
   ws->tuning = *tuning;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_set_graphs(clue_workspace* ws, int32_t enable) {
+  if (!ws)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");
+  ws->graphs = enable != 0;
+  if (!ws->graphs && ws->graph_exec) {
+    cudaSetDevice(ws->device);
+    if (ws->has_run)
+      cudaEventSynchronize(ws->run_event);
+    cudaGraphExecDestroy(ws->graph_exec);
+    ws->graph_exec = nullptr;
+  }
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_graph_replayed(const clue_workspace* ws, int32_t* replayed) {
+  if (!ws || !replayed)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  *replayed = ws->graph_replays_last ? 1 : 0;
   return CLUE_OK;
 }
 
@@ -816,6 +963,9 @@ clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* param
     if ((e = cudaEventCreate(&x)) != cudaSuccess)
       return fail_cuda(e, "cudaEventCreate");
   const clue_tuning start = ws->tuning;
+  // candidates run uncaptured: every one has its own tuning
+  const bool graphs = ws->graphs;
+  ws->graphs = false;
   // Median device time of `reps` runs under t, after one warm-up run.
   auto time_runs = [&](const clue_tuning& t, float* ms) -> clue_status {
     ws->tuning = t;
@@ -868,6 +1018,7 @@ clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* param
   for (auto& x : ev)
     cudaEventDestroy(x);
   ws->tuning = s == CLUE_OK ? best : start;
+  ws->graphs = graphs;
   if (s == CLUE_OK && chosen)
     *chosen = best;
   return s;

@@ -33,6 +33,20 @@ struct clue_workspace {
   const int32_t* last_labels = nullptr;  // device cluster ids of the last run
   int64_t last_launches = 0;             // kernels the last run enqueued
   clue_tuning tuning{};                  // launch choices (set at creation to the defaults)
+  // CUDA-graph replay (clue_workspace_set_graphs): the last run captured as a
+  // graph, and what it was captured for. A run with the same key replays it.
+  bool graphs = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  struct GraphKey {
+    clue_params params;
+    clue_points points;
+    clue_tuning tuning;
+    int32_t grid_mode = 0;
+    int64_t staged = 0;
+    char* base = nullptr;
+    std::vector<uint32_t> sizes;
+  } graph_key{};
+  bool graph_replays_last = false;  // whether the last run was a replay
 };
 
 namespace clue_impl {

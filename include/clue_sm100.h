@@ -150,6 +150,16 @@ size_t clue_workspace_bytes_for(int32_t ndim, int64_t n_points, int64_t n_tiles,
 #define CLUE_N_STAGES 6
 clue_status clue_workspace_set_profiling(clue_workspace* ws, int32_t enable);
 clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t capacity);
+/* CUDA-graph replay (off by default; no reference counterpart). When on, a
+ * device run on a non-default stream (without stage timing) is captured into a
+ * CUDA graph, and a later run with identical arguments — the same pointers,
+ * event sizes, parameters, grid mode and tuning — replays it: no host-side
+ * table building and one graph launch instead of ~20 kernel launches. The
+ * inputs' contents may change between replays. Any other run replaces the
+ * graph. Turning it off releases the graph. */
+clue_status clue_workspace_set_graphs(clue_workspace* ws, int32_t enable);
+/* 1 when the workspace's last run was a graph replay, else 0. */
+clue_status clue_workspace_graph_replayed(const clue_workspace* ws, int32_t* replayed);
 /* Number of CUDA kernels the last run on this workspace enqueued (no reference
  * counterpart; a check that the run executed on the GPU). */
 clue_status clue_workspace_kernel_launches(const clue_workspace* ws, int64_t* launches);

@@ -435,3 +435,46 @@ def test_autotune_keeps_results(batched):
                    grid_mode=clue.GRID_PER_EVENT)
     assert_identical(dict(rho=pts.rho.cpu().numpy(), nh=pts.nearest_higher.cpu().numpy(),
                           seed=pts.is_seed.cpu().numpy(), ci=pts.cluster_index.cpu().numpy()), o)
+
+
+# ---- CUDA-graph replay -------------------------------------------------------------------------
+
+def _device_outputs(pts):
+    return dict(rho=pts.rho.cpu().numpy(), nh=pts.nearest_higher.cpu().numpy(),
+                seed=pts.is_seed.cpu().numpy(), ci=pts.cluster_index.cpu().numpy())
+
+
+def test_graph_replay_reads_new_contents_and_recaptures_on_new_shapes():
+    import torch
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.Stream()
+    ev, sizes = W.batch_2d(32, 256, 8192, seed=51)
+    pts = clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev))
+    c = clue.Clusterer(1.5, 5.0, 1.5)
+    c.set_graphs(True)
+    kw = dict(batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=stream)
+    c.make_clusters(pts, **kw)
+    assert not c.graph_replayed()
+    first = _device_outputs(pts)
+    assert_identical(first, run_oracle(ev.coords, ev.weights, 1.5, 5.0, 1.5, sizes=sizes,
+                                       grid_mode=clue.GRID_PER_EVENT))
+    c.make_clusters(pts, **kw)
+    assert c.graph_replayed()
+    assert_identical(_device_outputs(pts), run_oracle(ev.coords, ev.weights, 1.5, 5.0, 1.5, sizes=sizes,
+                                                      grid_mode=clue.GRID_PER_EVENT))
+    # new weights in the same buffer (the events stop being exact-sum ones): the replay reads them
+    w2 = np.random.default_rng(52).exponential(1.0, ev.n).astype(np.float32)
+    pts.weights.copy_(torch.from_numpy(w2).to(dev))
+    c.make_clusters(pts, **kw)
+    assert c.graph_replayed()
+    assert_identical(_device_outputs(pts), run_oracle(ev.coords, w2, 1.5, 5.0, 1.5, sizes=sizes,
+                                                      grid_mode=clue.GRID_PER_EVENT))
+    # other event sizes over the same points: captured again
+    sizes2 = np.array([ev.n // 2, ev.n - ev.n // 2], np.uint32)
+    c.make_clusters(pts, batch_item_sizes=sizes2, grid_mode=clue.GRID_PER_EVENT, stream=stream)
+    assert not c.graph_replayed()
+    assert_identical(_device_outputs(pts), run_oracle(ev.coords, w2, 1.5, 5.0, 1.5, sizes=sizes2,
+                                                      grid_mode=clue.GRID_PER_EVENT))
+    c.set_graphs(False)
+    c.make_clusters(pts, batch_item_sizes=sizes2, grid_mode=clue.GRID_PER_EVENT, stream=stream)
+    assert not c.graph_replayed()
