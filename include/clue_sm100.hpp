@@ -761,6 +761,33 @@ class Clusterer {
     finish(q, d);
   }
 
+  // No reference counterpart: CUDA-graph replay of repeated identical device
+  // runs, launch tuning and the autotuner (clue_workspace_set_graphs,
+  // clue_workspace_{get,set}_tuning, clue_workspace_autotune). Results do not
+  // depend on any of them.
+  void set_graphs(Queue& q, bool enable) {
+    detail::check(clue_workspace_set_graphs(workspace(q.device()), enable ? 1 : 0));
+  }
+  clue_tuning tuning(Queue& q) {
+    clue_tuning t{};
+    detail::check(clue_workspace_get_tuning(workspace(q.device()), &t));
+    return t;
+  }
+  void set_tuning(Queue& q, const clue_tuning& t) {
+    detail::check(clue_workspace_set_tuning(workspace(q.device()), &t));
+  }
+  template <typename TIn, typename Metric = EuclideanMetric<Ndim>, typename Kernel = FlatKernel<>>
+  clue_tuning autotune(Queue& q, PointsDevice<Ndim, TIn>& d, const Metric& metric = Metric{},
+                       const Kernel& kernel = FlatKernel<>{.5f}, int32_t reps = 3) {
+    const clue_params p = with(metric, kernel);
+    const clue_points pts = d.abi();
+    clue_tuning t{};
+    detail::check(clue_workspace_autotune(workspace(q.device()), &p, &pts, nullptr, 0, 0, q.stream(), reps,
+                                          &t));
+    finish(q, d);
+    return t;
+  }
+
   // getSeeds (:197-203): seed indices of the last run; cluster id k is seeds[k].
   std::span<const int32_t> getSeeds() {
     if (!ws_)
@@ -830,5 +857,148 @@ class Clusterer {
   int32_t batch_size_ = 1;
   std::vector<int32_t> seeds_;
 };
+
+// ---------------------------------------------------------------------------
+// Validation utilities (utils/cluster_centroid.hpp, utils/scores.hpp): the
+// reference's host functions over a clustered PointsHost, computed on GPU 0
+// (clue_cluster_centroids_device, clue_silhouette_device) from temporary
+// device copies of the points and of their cluster map.
+// ---------------------------------------------------------------------------
+
+template <std::size_t Ndim, typename ValueType = float>
+using Centroid = std::array<std::remove_cv_t<ValueType>, Ndim>;
+template <std::size_t Ndim, typename ValueType = float>
+using Centroids = std::vector<Centroid<Ndim, ValueType>>;
+
+namespace detail {
+
+// Device copies of a clustered host point set (coordinates, weights, labels)
+// and of its cluster map; released when the object goes.
+template <std::size_t Ndim>
+class DeviceClusters {
+ public:
+  template <typename T>
+  explicit DeviceClusters(const PointsHost<Ndim, T>& h) : q_{get_device(0)} {
+    if (!h.clustered())
+      throw std::runtime_error("the points have not been clustered");
+    const clue_points hp = h.abi();
+    const std::size_t n = static_cast<std::size_t>(h.size());
+    map_ = AssociationMapHost::from_keys(h.clusterIndexes());
+    pts_.ndim = static_cast<int32_t>(Ndim);
+    pts_.n = h.size();
+    for (std::size_t d = 0; d < Ndim; ++d)
+      pts_.coords[d] = static_cast<const float*>(upload(hp.coords[d], n * 4));
+    pts_.weight = static_cast<const float*>(upload(hp.weight, n * 4));
+    pts_.cluster_index = static_cast<int32_t*>(upload(h.clusterIndexes().data(), n * 4));
+    offsets_ = static_cast<int32_t*>(upload(map_.offsets().data(), map_.offsets().size() * 4));
+    members_ = static_cast<int32_t*>(upload(map_.values().data(), map_.values().size() * 4));
+  }
+  DeviceClusters(const DeviceClusters&) = delete;
+  DeviceClusters& operator=(const DeviceClusters&) = delete;
+  ~DeviceClusters() {
+    clue_stream_synchronize(q_.stream());
+    for (void* p : bufs_)
+      clue_device_free(p);
+  }
+
+  int32_t n_clusters() const { return static_cast<int32_t>(map_.size()); }
+
+  // n_clusters x Ndim, row-major
+  std::vector<float> centroids(bool weighted) {
+    const std::size_t k = static_cast<std::size_t>(n_clusters());
+    std::vector<float> out(k * Ndim);
+    if (k == 0)
+      return out;
+    auto* d_out = static_cast<float*>(alloc(out.size() * 4));
+    check(clue_cluster_centroids_device(&pts_, offsets_, members_, n_clusters(), weighted ? 1 : 0, d_out,
+                                        q_.stream()));
+    check(clue_memcpy_async(out.data(), d_out, out.size() * 4, 1, q_.stream()));
+    q_.wait();
+    return out;
+  }
+
+  // per point; NaN where the reference's mean skips the point
+  std::vector<float> silhouettes() {
+    std::vector<float> out(static_cast<std::size_t>(pts_.n));
+    auto* d_out = static_cast<float*>(alloc(out.size() * 4));
+    check(clue_silhouette_device(&pts_, offsets_, members_, n_clusters(), d_out, q_.stream()));
+    check(clue_memcpy_async(out.data(), d_out, out.size() * 4, 1, q_.stream()));
+    q_.wait();
+    return out;
+  }
+
+ private:
+  void* alloc(std::size_t bytes) {
+    void* p = nullptr;
+    check(clue_device_malloc(&p, std::max<std::size_t>(bytes, 4), q_.device()));
+    bufs_.push_back(p);
+    return p;
+  }
+  void* upload(const void* src, std::size_t bytes) {
+    void* p = alloc(bytes);
+    if (bytes)
+      check(clue_memcpy_async(p, src, bytes, 0, q_.stream()));
+    return p;
+  }
+
+  Queue q_;
+  AssociationMapHost map_;
+  clue_points pts_{};
+  int32_t* offsets_ = nullptr;
+  int32_t* members_ = nullptr;
+  std::vector<void*> bufs_;
+};
+
+template <std::size_t Ndim>
+Centroids<Ndim> to_centroids(const std::vector<float>& flat) {
+  Centroids<Ndim> out(flat.size() / Ndim);
+  for (std::size_t c = 0; c < out.size(); ++c)
+    std::copy_n(flat.begin() + static_cast<std::ptrdiff_t>(c * Ndim), Ndim, out[c].begin());
+  return out;
+}
+
+}  // namespace detail
+
+// cluster_centroids / weighted_cluster_centroids (utils/detail/cluster_centroid.hpp:86-140)
+template <std::size_t Ndim, typename T>
+Centroids<Ndim> cluster_centroids(const PointsHost<Ndim, T>& points) {
+  detail::DeviceClusters<Ndim> dc(points);
+  return detail::to_centroids<Ndim>(dc.centroids(false));
+}
+template <std::size_t Ndim, typename T>
+Centroids<Ndim> weighted_cluster_centroids(const PointsHost<Ndim, T>& points) {
+  detail::DeviceClusters<Ndim> dc(points);
+  return detail::to_centroids<Ndim>(dc.centroids(true));
+}
+// cluster_centroid / weighted_cluster_centroid (:16-84): zeros for a cluster
+// with no points.
+template <std::size_t Ndim, typename T>
+Centroid<Ndim> cluster_centroid(const PointsHost<Ndim, T>& points, std::size_t cluster_id) {
+  const auto all = cluster_centroids(points);
+  return cluster_id < all.size() ? all[cluster_id] : Centroid<Ndim>{};
+}
+template <std::size_t Ndim, typename T>
+Centroid<Ndim> weighted_cluster_centroid(const PointsHost<Ndim, T>& points, std::size_t cluster_id) {
+  const auto all = weighted_cluster_centroids(points);
+  return cluster_id < all.size() ? all[cluster_id] : Centroid<Ndim>{};
+}
+
+// silhouette(points, point) and silhouette(points) (utils/detail/scores.hpp:33-100);
+// the mean is the reference's std::reduce over the points it keeps.
+template <std::size_t Ndim, typename T>
+float silhouette(const PointsHost<Ndim, T>& points, std::size_t point) {
+  detail::DeviceClusters<Ndim> dc(points);
+  return dc.silhouettes().at(point);
+}
+template <std::size_t Ndim, typename T>
+float silhouette(const PointsHost<Ndim, T>& points) {
+  detail::DeviceClusters<Ndim> dc(points);
+  const std::vector<float> all = dc.silhouettes();
+  std::vector<float> scores;
+  for (float s : all)
+    if (s == s)
+      scores.push_back(s);
+  return std::reduce(scores.begin(), scores.end(), 0.0f) / static_cast<float>(scores.size());
+}
 
 }  // namespace clue

@@ -1,11 +1,13 @@
 // C++ API checks, written like CLUEstering's doctest cases. Exit code 0 when
 // every CHECK holds. argv[1]: a float32 file of the 10 x 1024-point batch
 // (x planes then y then weights); argv[2]: data_32768 in the same layout;
-// argv[3]: output file for the cluster ids of every make_clusters overload.
+// argv[3]: output file for the cluster ids of every make_clusters overload
+// (argv[3] + ".util": centroids and silhouettes of the last one).
 #include <cstdio>
 #include <fstream>
 #include <iostream>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "CLUEstering/CLUEstering.hpp"
@@ -169,6 +171,48 @@ int main(int argc, char** argv) {
       clue::PointsHost<2> h(queue, n, x.data(), y.data(), w.data(), ids.data());
       algo.make_clusters(queue, h);
       dump(h);
+      // utils/cluster_centroid.hpp and utils/scores.hpp, written for the checker:
+      // k, k x 2 centroids, k x 2 weighted centroids, the mean silhouette and the
+      // silhouette of the first clustered point with its index
+      const auto cen = clue::cluster_centroids(h);
+      const auto wcen = clue::weighted_cluster_centroids(h);
+      CHECK(cen.size() == h.n_clusters() && wcen.size() == cen.size());
+      CHECK(clue::cluster_centroid(h, 0) == cen[0]);
+      CHECK(clue::weighted_cluster_centroid(h, cen.size()) == (clue::Centroid<2>{}));
+      int first = 0;
+      while (ids[first] < 0)
+        ++first;
+      const float sil = clue::silhouette(h);
+      const float sil_first = clue::silhouette(h, static_cast<std::size_t>(first));
+      std::ofstream util(std::string(argv[3]) + ".util", std::ios::binary);
+      const float k = static_cast<float>(cen.size());
+      util.write(reinterpret_cast<const char*>(&k), 4);
+      for (const auto& c : cen)
+        util.write(reinterpret_cast<const char*>(c.data()), 8);
+      for (const auto& c : wcen)
+        util.write(reinterpret_cast<const char*>(c.data()), 8);
+      const float tail[3] = {sil, sil_first, static_cast<float>(first)};
+      util.write(reinterpret_cast<const char*>(tail), 12);
+    }
+    {  // CUDA-graph replay and the autotuner leave the result as it is
+      std::vector<int> ids(n);
+      clue::PointsHost<2> h(queue, n, data.data(), ids.data());
+      clue::PointsDevice<2> d(queue, n);
+      clue::copyToDevice(queue, d, h);
+      clue::Clusterer<2> tuned(queue, 1.3f, 10.f, 1.3f);
+      tuned.autotune(queue, d, clue::EuclideanMetric<2>{}, clue::FlatKernel<>{.5f}, 1);
+      tuned.set_graphs(queue, true);
+      for (int r = 0; r < 2; ++r) {
+        tuned.make_clusters(queue, d);
+        std::vector<int> again(n);
+        clue_memcpy_async(again.data(), d.clusterIndexes(), n * 4, 1, queue.stream());
+        queue.wait();
+        std::vector<int> plain(n);
+        clue::PointsHost<2> h2(queue, n, data.data(), plain.data());
+        algo.make_clusters(queue, h2);
+        CHECK(again == plain);
+      }
+      CHECK(tuned.tuning(queue).label_jump_rounds >= -1);
     }
   }
   if (failures)

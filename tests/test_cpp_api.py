@@ -53,3 +53,15 @@ def test_cpp_api_known_answers_and_overloads(tmp_path):
     assert ids.shape[0] == 5
     for row in ids:
         assert np.array_equal(row, ref)
+    # clue::cluster_centroids, weighted_cluster_centroids and silhouette on the last overload's result
+    util = np.fromfile(str(out) + ".util", np.float32)
+    k = int(util[0])
+    assert k == int(ref.max()) + 1
+    cen, wcen = util[1:1 + 2 * k].reshape(k, 2), util[1 + 2 * k:1 + 4 * k].reshape(k, 2)
+    assert np.array_equal(cen.view(np.int32), O.centroids(c, w, ref, k).view(np.int32))
+    assert np.array_equal(wcen.view(np.int32), O.centroids(c, w, ref, k, weighted=True).view(np.int32))
+    sil, sil_first, first = util[1 + 4 * k:]
+    scores = O.silhouette(c, ref, k)
+    assert sil_first == scores[int(first)]
+    # the mean is a float std::reduce over ~30,000 scores, as in the reference: float accuracy
+    assert sil == pytest.approx(float(np.mean(scores[~np.isnan(scores)].astype(np.float64))), rel=1e-5)
