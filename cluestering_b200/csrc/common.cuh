@@ -256,6 +256,44 @@ __device__ __forceinline__ float kernel_value_in_range(const RunParams& p, float
   return p.kernel_p0;
 }
 
+// ---------------------------------------------------------------------------
+// Exact-sum events (flat kernel)
+//
+// The reference adds a point's density contributions in its tile order, and
+// float addition rounds, so in general only that order reproduces its bits.
+// When every contribution of an event (fl(flat * w_j) for a neighbour, w_i for
+// the point itself) is a non-negative integer multiple of u = 2^min_lsb and
+// their total over the event is at most 2^24 u, every partial sum of any subset
+// is an integer multiple of u no larger than 2^24 u, which binary32 represents
+// exactly: no addition rounds, and the ordered sum equals the exact sum in any
+// order (unit weights are the common case: multiples of 1/2). k_bin records per
+// event (4 ints): the smallest lowest-set-bit exponent of any contribution, the
+// largest neighbour contribution and the largest weight (float bits), and a
+// flag for a negative, -0, NaN or infinite one.
+// ---------------------------------------------------------------------------
+
+// Exponent of the lowest set bit of a positive finite float: x = m * 2^e with
+// m odd returns e.
+__device__ __forceinline__ int lsb_exponent(float x) {
+  const uint32_t bits = __float_as_uint(x);
+  const uint32_t ex = (bits >> 23) & 0xffu;
+  const uint32_t m = ex ? ((bits & 0x7fffffu) | 0x800000u) : (bits & 0x7fffffu);
+  return (ex ? (int)ex - 150 : -149) + (__ffs(m) - 1);
+}
+
+// The bound is checked in double: the true bound n * max_v + max_w and 2^24 u
+// are multiples of u, so a true bound above 2^24 u is at least (2^24 + 1) u,
+// which the double product cannot round down to 2^24 u.
+__device__ __forceinline__ bool event_sums_exact(const int32_t* event_exact, int e, int n_points) {
+  const int4 st = reinterpret_cast<const int4*>(event_exact)[e];
+  if (st.w != 0)
+    return false;
+  if (st.x == INT_MAX)
+    return true;  // every contribution is zero
+  const double bound = (double)n_points * (double)__int_as_float(st.y) + (double)__int_as_float(st.z);
+  return bound <= ldexp(1.0, 24 + st.x);
+}
+
 // Status word bits written by kernels whose waits are bounded.
 enum : uint32_t {
   kStatusScanTimeout = 1u << 0,

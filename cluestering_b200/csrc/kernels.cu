@@ -64,12 +64,15 @@ __device__ float fmax_op(float a, float b) { return fmaxf(a, b); }
 // Grid extents: core/detail/ComputeTiles.hpp:16-62, SetupTiles.hpp:19-96
 // ---------------------------------------------------------------------------
 
-__global__ void k_grid_init(int32_t* grid_minmax, int n_grids) {
+__global__ void k_grid_init(int32_t* grid_minmax, int n_grids, int32_t* event_exact, int n_events) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n_grids * kMaxDim) {
     grid_minmax[2 * i] = f2ord(FLT_MAX);       // min starts at numeric_limits::max()
     grid_minmax[2 * i + 1] = f2ord(-FLT_MAX);  // max starts at numeric_limits::lowest()
   }
+  // exact-sum bounds (common.cuh), filled by k_bin
+  if (event_exact && i < 4 * n_events)
+    event_exact[i] = (i & 3) == 0 ? INT_MAX : 0;
 }
 
 __global__ void __launch_bounds__(kThreads) k_minmax(int D, CoordPtrs x, const Chunk* chunks,
@@ -113,10 +116,14 @@ __global__ void k_grid_finalize(int D, GridDesc* grids, int n_grids, const int32
 // Tiles::GetGlobalBin (Tiles.hpp:208-227, TilesView.hpp:54-64)
 // ---------------------------------------------------------------------------
 
+// Also the exact-sum bounds of the chunk's event (flat kernel, when
+// event_exact is given): lowest-bit exponent, largest contributions, and a flag
+// for a negative, -0, NaN or infinite weight, one atomic per warp.
 __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, const Chunk* chunks,
                                                   const EventDesc* events, const GridDesc* grids,
                                                   int32_t* tile_of, int32_t* point_event,
-                                                  int32_t* tile_count) {
+                                                  int32_t* tile_count, const float* weight,
+                                                  int32_t* event_exact) {
   __shared__ GridDesc sg;
   const Chunk c = chunks[blockIdx.x];
   const EventDesc ev = events[c.event];
@@ -140,6 +147,35 @@ __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, cons
     const int leader = __ffs(mask) - 1;
     if (valid && lane == leader)
       atomicAdd(&tile_count[t], __popc(mask));
+    if (event_exact && p.kernel_kind == CLUE_KERNEL_FLAT) {  // block-uniform
+      int lsb = INT_MAX, bad = 0;
+      uint32_t vb = 0, wb = 0;
+      if (valid) {
+        const float w = weight[i];
+        const float v = __fmul_rn(p.kernel_p0, w);  // a neighbour's fl(flat * w_j)
+        bad = !(w >= 0.0f) || signbit(w) || isinf(w) || isinf(v);
+        if (!bad) {
+          if (v > 0.0f)
+            lsb = min(lsb, lsb_exponent(v));
+          if (w > 0.0f)
+            lsb = min(lsb, lsb_exponent(w));
+          vb = __float_as_uint(v);
+          wb = __float_as_uint(w);
+        }
+      }
+      lsb = __reduce_min_sync(kFull, lsb);
+      vb = __reduce_max_sync(kFull, vb);
+      wb = __reduce_max_sync(kFull, wb);
+      bad = __any_sync(kFull, bad);
+      if (lane == 0) {
+        int32_t* st = event_exact + 4 * c.event;
+        atomicMin(&st[0], lsb);
+        atomicMax(reinterpret_cast<unsigned*>(&st[1]), vb);
+        atomicMax(reinterpret_cast<unsigned*>(&st[2]), wb);
+        if (bad)
+          atomicOr(&st[3], 1);
+      }
+    }
   }
 }
 
@@ -386,14 +422,29 @@ __device__ __forceinline__ void warp_rank_sort(int32_t* seg, int m, int* ids, in
       seg[r[k]] = v[k];
 }
 
+// Whether the ids of the segment starting at `begin` may stay in any order:
+// with `event_exact` given, the segment is a tile of an event whose density
+// sums are exact in any order (common.cuh), the only use of the ascending
+// order within a tile on this run.
+__device__ __forceinline__ bool order_free(const int32_t* event_exact, const int32_t* point_event,
+                                          const EventDesc* events, const int32_t* perm, int begin) {
+  if (!event_exact)
+    return false;
+  const int e = point_event[perm[begin]];
+  return event_sums_exact(event_exact, e, events[e].n);
+}
+
 // Orders the ids of every tile ascending. One warp per tile: tiles of up to
 // kWarpSortCap ids are rank-sorted by the warp with no block barrier; larger
-// tiles are listed for k_tile_sort_large. Tiles already in order (one warp of
-// the scatter placed all of them) are left as they are.
+// tiles are listed for k_tile_sort_large (and for k_cells, which gives each a
+// block). Tiles already in order (one warp of the scatter placed all of them)
+// and tiles whose order does not matter (order_free) are left as they are.
 constexpr int kWarpSortCap = kLargeTilePoints;
 __global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offset, int64_t n_tiles,
                                                         int32_t* perm, int32_t* large,
-                                                        int32_t* large_count) {
+                                                        int32_t* large_count, const int32_t* event_exact,
+                                                        const int32_t* point_event,
+                                                        const EventDesc* events) {
   __shared__ __align__(16) int s_ids[kThreads / 32][kWarpSortCap];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* ids = s_ids[warp];
@@ -408,6 +459,8 @@ __global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offs
         large[atomicAdd(large_count, 1)] = (int32_t)t;
       continue;
     }
+    if (order_free(event_exact, point_event, events, perm, begin))
+      continue;
     int unsorted = 0;
     for (int i = lane; i < m; i += 32) {
       const int v = perm[begin + i];
@@ -491,14 +544,17 @@ __global__ void __launch_bounds__(kThreads) k_tile_sort_large(const int32_t* til
                                                               const int32_t* large,
                                                               const int32_t* large_count,
                                                               int32_t* perm, int32_t* oversize,
-                                                              int32_t* oversize_count) {
+                                                              int32_t* oversize_count,
+                                                              const int32_t* event_exact,
+                                                              const int32_t* point_event,
+                                                              const EventDesc* events) {
   __shared__ int s[kSortCap];
   const int count = *large_count;
   for (int e = blockIdx.x; e < count; e += gridDim.x) {
     const int t = large[e];
     const int begin = tile_offset[t], end = tile_offset[t + 1];
     const int m = end - begin;
-    if (m <= 1)
+    if (m <= 1 || order_free(event_exact, point_event, events, perm, begin))
       continue;
     if (m <= kChunkRankCap) {
       chunk_rank_sort(perm + begin, m, s);
@@ -676,8 +732,10 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
 }
 
 // Sorts ids[offsets[k] .. offsets[k + 1]) ascending for every segment k.
+// With `event_exact`, segments are tiles and those of exact-sum events keep
+// their order (order_free).
 cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* ids,
-                          const DeviceBuffers& b, cudaStream_t st) {
+                          const DeviceBuffers& b, cudaStream_t st, const int32_t* event_exact = nullptr) {
   int32_t* oversize_count = b.counters + 2;
   int32_t* large_count = b.counters + 3;
   cudaError_t e = cudaMemsetAsync(oversize_count, 0, 2 * sizeof(int32_t), st);
@@ -687,9 +745,11 @@ cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* i
   const int blocks =
       (int)std::max<int64_t>(1, std::min<int64_t>((n_segments + warps_per_block - 1) / warps_per_block,
                                                   148 * 16));
-  k_tile_sort<<<blocks, kThreads, 0, st>>>(offsets, n_segments, ids, b.large_tiles, large_count);
+  k_tile_sort<<<blocks, kThreads, 0, st>>>(offsets, n_segments, ids, b.large_tiles, large_count,
+                                           event_exact, b.point_event, b.events);
   k_tile_sort_large<<<148 * 8, kThreads, 0, st>>>(offsets, b.large_tiles, large_count, ids,
-                                                  b.oversize, oversize_count);
+                                                  b.oversize, oversize_count, event_exact,
+                                                  b.point_event, b.events);
   k_tile_merge<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, ids, b.merge_tmp);
   k_tile_merge_copy<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, b.merge_tmp,
                                               ids);
@@ -775,7 +835,11 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // grid extents
   CLUE_MARK(0);
-  k_grid_init<<<(sh.n_grids * kMaxDim + 127) / 128, 128, 0, st>>>(b.grid_minmax, sh.n_grids);
+  // exact-sum bounds per event (2-D and 3-D runs: their workspace holds them)
+  int32_t* exact = (D == 2 || D == 3) ? b.event_exact : nullptr;
+  const int64_t init_items = std::max<int64_t>((int64_t)sh.n_grids * kMaxDim, exact ? 4 * (int64_t)sh.n_events : 0);
+  k_grid_init<<<(int)((init_items + 127) / 128), 128, 0, st>>>(b.grid_minmax, sh.n_grids, exact,
+                                                               sh.n_events);
   CLUE_LAUNCHED();
   k_minmax<<<sh.n_chunks, kThreads, 0, st>>>(D, x, b.chunks, b.events, b.grid_minmax);
   CLUE_LAUNCHED();
@@ -786,14 +850,17 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   CLUE_MARK(1);
   CLUE_CHECK(cudaMemsetAsync(b.tile_count, 0, sizeof(int32_t) * sh.n_tiles, st));
   k_bin<<<sh.n_chunks, kThreads, 0, st>>>(prm, x, b.chunks, b.events, b.grids, b.tile_of,
-                                           b.point_event, b.tile_count);
+                                           b.point_event, b.tile_count, io.weight, exact);
   CLUE_LAUNCHED();
   CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));
   CLUE_CHECK(cudaMemcpyAsync(b.tile_cursor, b.tile_offset, sizeof(int32_t) * sh.n_tiles,
                              cudaMemcpyDeviceToDevice, st));
   k_scatter<<<grid_for(n), kThreads, 0, st>>>(b.tile_of, n, b.tile_cursor, b.perm);
   CLUE_LAUNCHED();
-  CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st));
+  // Exact-sum events need no ascending order within their tiles when nothing
+  // else on this run reads it (flat kernel, cell path: no user tags).
+  const bool order_free_tiles = sweep_cells_path(prm) && prm.kernel_kind == CLUE_KERNEL_FLAT;
+  CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st, order_free_tiles ? exact : nullptr));
   CLUE_MARK(2);
   k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
                                              io.unc, io.tags, b.point_event, b.sorted_coords,

@@ -363,85 +363,30 @@ __device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
   return __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
 }
 
-// Exponent of the lowest set bit of a positive finite float: x = m * 2^e with
-// m odd returns e.
-__device__ __forceinline__ int lsb_exponent(float x) {
-  const uint32_t bits = __float_as_uint(x);
-  const uint32_t ex = (bits >> 23) & 0xffu;
-  const uint32_t m = ex ? ((bits & 0x7fffffu) | 0x800000u) : (bits & 0x7fffffu);
-  return (ex ? (int)ex - 150 : -149) + (__ffs(m) - 1);
-}
-
 // Density records, in sorted order and (with the cell layout) in cell-layout
-// order. For the flat kernel also the per-event bounds of event_sums_exact:
-// the smallest lowest-bit exponent of any contribution (a neighbour's
-// fl(flat * w_j), the point's own w_i), the largest of each, and whether any
-// weight is negative, -0, NaN or infinite.
+// order.
 template <int D>
 __global__ void __launch_bounds__(kThreads) k_pack_density(const RunParams p, const SweepArgs a) {
   if (blockIdx.x == 0 && threadIdx.x < 2)
     a.queue[threadIdx.x] = 0;  // the sweeps that follow start with no item taken
-  const bool stats = p.kernel_kind == CLUE_KERNEL_FLAT && a.event_exact != nullptr;
-  const int lane = threadIdx.x & 31;
-  // every lane of a warp runs the same iterations (warp reductions below)
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < a.n; base += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t s = base + threadIdx.x;
-    const bool valid = s < a.n;
-    int e = -1, lsb = INT_MAX, bad = 0;
-    uint32_t vb = 0, wb = 0;
-    if (valid) {
-      const float w = a.sw[s];
-      // flat: contribution of a neighbour is fl(flat * w_j) (ConvolutionalKernel.hpp:24-27)
-      const float v = p.kernel_kind == CLUE_KERNEL_FLAT ? __fmul_rn(p.kernel_p0, w) : w;
-      float4 r;
-      r.x = a.sx[s];
-      r.y = a.sx[a.n + s];
-      if (D == 2) {
-        r.z = v;
-        r.w = w;
-      } else {
-        r.z = a.sx[2 * a.n + s];
-        r.w = v;
-      }
-      a.rec_dens[s] = r;
-      if (a.rec_cell)
-        a.rec_cell[a.nh_pos[s]] = r;
-      if (stats) {
-        e = a.sevt[s];
-        bad = !(w >= 0.0f) || signbit(w) || isinf(w) || isinf(v);
-        if (!bad) {
-          if (v > 0.0f)
-            lsb = min(lsb, lsb_exponent(v));
-          if (w > 0.0f)
-            lsb = min(lsb, lsb_exponent(w));
-          vb = __float_as_uint(v);
-          wb = __float_as_uint(w);
-        }
-      }
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const float w = a.sw[s];
+    // flat: contribution of a neighbour is fl(flat * w_j) (ConvolutionalKernel.hpp:24-27)
+    const float v = p.kernel_kind == CLUE_KERNEL_FLAT ? __fmul_rn(p.kernel_p0, w) : w;
+    float4 r;
+    r.x = a.sx[s];
+    r.y = a.sx[a.n + s];
+    if (D == 2) {
+      r.z = v;
+      r.w = w;
+    } else {
+      r.z = a.sx[2 * a.n + s];
+      r.w = v;
     }
-    if (!stats)
-      continue;
-    int32_t* st = a.event_exact;
-    const int e0 = __shfl_sync(kFullMask, e, 0);
-    if (__all_sync(kFullMask, !valid || e == e0)) {
-      lsb = __reduce_min_sync(kFullMask, lsb);
-      vb = __reduce_max_sync(kFullMask, vb);
-      wb = __reduce_max_sync(kFullMask, wb);
-      bad = __any_sync(kFullMask, bad);
-      if (lane == 0 && e0 >= 0) {
-        atomicMin(&st[4 * e0], lsb);
-        atomicMax(reinterpret_cast<unsigned*>(&st[4 * e0 + 1]), vb);
-        atomicMax(reinterpret_cast<unsigned*>(&st[4 * e0 + 2]), wb);
-        if (bad)
-          atomicOr(&st[4 * e0 + 3], 1);
-      }
-    } else if (valid) {
-      atomicMin(&st[4 * e], lsb);
-      atomicMax(reinterpret_cast<unsigned*>(&st[4 * e + 1]), vb);
-      atomicMax(reinterpret_cast<unsigned*>(&st[4 * e + 2]), wb);
-      if (bad)
-        atomicOr(&st[4 * e + 3], 1);
-    }
+    a.rec_dens[s] = r;
+    if (a.rec_cell)
+      a.rec_cell[a.nh_pos[s]] = r;
   }
 }
 
@@ -716,37 +661,15 @@ __device__ __forceinline__ unsigned range_bits(int lo, int hi) {
 }
 
 // ---------------------------------------------------------------------------
-// Exact-sum density (flat kernel).
-//
-// The reference adds a point's contributions in its tile order, and float
-// addition rounds, so in general only that order reproduces its bits. When
-// every contribution of an event (fl(flat * w_j) for a neighbour, w_i for the
-// point itself) is a non-negative integer multiple of u = 2^min_lsb and their
-// total over the event is at most 2^24 u, every partial sum of any subset is
-// an integer multiple of u no larger than 2^24 u, which binary32 represents
-// exactly: no addition rounds, and the ordered sum equals the exact sum in any
-// order (unit weights are the common case: multiples of 1/2). Such events skip
-// the ordered stream: a warp streams only the cells within reach of its 32
-// points, and each lane adds its in-range candidates from its own box's tiles,
-// the same candidate set as the reference's.
+// Exact-sum density (flat kernel; event_sums_exact in common.cuh). For an
+// event whose sums are exact in any order, a warp streams only the cells
+// within reach of its 32 points, and each lane adds its in-range candidates
+// from its own box's tiles, the same candidate set as the reference's.
 // ---------------------------------------------------------------------------
 
 constexpr int kMaxSegs = 64;        // cell-row segments an exact-sum warp streams (2 per lane)
 constexpr int kMaxUnionTiles = 32;  // tiles of the warp's union box (one per lane)
 constexpr int kMaxStream = kMaxSegs > kMaxRows ? kMaxSegs : kMaxRows;
-
-// The bound is checked in double: the true bound n * max_v + max_w and 2^24 u
-// are multiples of u, so a true bound above 2^24 u is at least (2^24 + 1) u,
-// which the double product cannot round down to 2^24 u.
-__device__ __forceinline__ bool event_sums_exact(const SweepArgs& a, int e, int n_points) {
-  const int4 st = reinterpret_cast<const int4*>(a.event_exact)[e];
-  if (st.w != 0)
-    return false;
-  if (st.x == INT_MAX)
-    return true;  // every contribution is zero
-  const double bound = (double)n_points * (double)__int_as_float(st.y) + (double)__int_as_float(st.z);
-  return bound <= ldexp(1.0, 24 + st.x);
-}
 
 // One warp, exact-sum event. Returns false (nothing done) when the warp's
 // reach needs more than kMaxSegs segments or kMaxUnionTiles tiles; the caller
@@ -1050,7 +973,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p,
     float rho = 0.0f;
     // events whose sums are exact in any order stream only the cells in reach
     const bool exact = KIND == CLUE_KERNEL_FLAT && a.rec_cell != nullptr && one_grid && u_ordered &&
-                       __all_sync(kFullMask, event_sums_exact(a, a.sevt[s], ev.n));
+                       __all_sync(kFullMask, event_sums_exact(a.event_exact, a.sevt[s], ev.n));
     bool done = false;  // warp-uniform: the exact-sum path handled the warp
     if (exact)
       done = density_exact<D>(p, a, ev, g, xi, s, wi, inf, sup, ordered, uinf, usup, ring, off, qa,
@@ -1569,11 +1492,6 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
   __shared__ int s_cnt2[kCellSlots];
   __shared__ int s_cls[kCellWarps][E];
   const int warp = threadIdx.x >> 5;
-  // per-event bounds of the exact-sum test, filled by k_pack_density
-  if (a.event_exact)
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 4 * (int64_t)a.n_events;
-         i += (int64_t)gridDim.x * blockDim.x)
-      a.event_exact[i] = (i & 3) == 0 ? INT_MAX : 0;
   if ((int)blockIdx.x < warp_blocks) {
     const int64_t stride = (int64_t)warp_blocks * kCellWarps;
     for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
