@@ -110,6 +110,7 @@ SIGNATURES = {
     "clue_workspace_stage_ms": (C.c_int, [_P, _P, C.c_int32]),
     "clue_workspace_kernel_launches": (C.c_int, [_P, _P]),
     "clue_workspace_set_graphs": (C.c_int, [_P, C.c_int32]),
+    "clue_selftest_bounded_wait": (C.c_int, [C.c_int32, _P]),
     "clue_workspace_graph_replayed": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "clue_tuning_defaults": (C.c_int, [C.POINTER(Tuning)]),
     "clue_workspace_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),

@@ -849,6 +849,31 @@ clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tun
   return CLUE_OK;
 }
 
+clue_status clue_selftest_bounded_wait(int32_t device, void* stream) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "cudaSetDevice");
+  // a zeroed descriptor (nothing ever publishes it) and a status word
+  void* buf = nullptr;
+  if ((e = cudaMalloc(&buf, 16)) != cudaSuccess)
+    return fail_cuda(e, "self-test allocation");
+  auto* desc = static_cast<unsigned long long*>(buf);
+  auto* status = reinterpret_cast<uint32_t*>(desc + 1);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  uint32_t host_status = 0;
+  if ((e = cudaMemsetAsync(buf, 0, 16, st)) == cudaSuccess &&
+      (e = launch_wait_probe(desc, status, st)) == cudaSuccess &&
+      (e = cudaMemcpyAsync(&host_status, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) ==
+          cudaSuccess)
+    e = cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "bounded-wait self-test");
+  if (host_status & kStatusScanTimeout)
+    return fail(CLUE_ERR_TIMEOUT, "the bounded wait gave up and reported it (expected)");
+  return fail(CLUE_ERR_RUNTIME, "the bounded wait did not report giving up");
+}
+
 clue_status clue_workspace_set_graphs(clue_workspace* ws, int32_t enable) {
   if (!ws)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "workspace is null");

@@ -135,6 +135,9 @@ cudaError_t launch_run(const RunShape& shape, const RunParams& prm, const RunIO&
 // Turns the batch-wide results of a run into per-event results: cluster ids
 // restart at 0 in every event and nearest-higher ids become event-local, which
 // is exactly what each event gets when clustered alone.
+// Runs the tile scan's bounded wait on `desc` (zeroed: nothing publishes it);
+// the kernel sets a bit in `status` when the wait gives up.
+cudaError_t launch_wait_probe(unsigned long long* desc, uint32_t* status, cudaStream_t stream);
 cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
                             int32_t* cluster_index, int32_t* nh, cudaStream_t stream);
 

@@ -199,6 +199,31 @@ __device__ __forceinline__ unsigned long long peek(unsigned long long* d) {
   return r.load(cuda::memory_order_acquire);
 }
 
+// Waits until descriptor d carries a flag, at most kSpinLimit polls; on giving
+// up it records kStatusScanTimeout in the status word and returns an
+// inclusive zero, so the scan finishes (with a wrong prefix the host then
+// reports as CLUE_ERR_TIMEOUT) instead of hanging.
+__device__ __forceinline__ unsigned long long await_descriptor(unsigned long long* d, uint32_t* status) {
+  int spins = 0;
+  unsigned long long dsc = peek(d);
+  while ((dsc >> 62) == 0) {
+    if (++spins > kSpinLimit) {
+      atomicOr(status, kStatusScanTimeout);
+      return kFlagInclusive;
+    }
+    __nanosleep(64);
+    dsc = peek(d);
+  }
+  return dsc;
+}
+
+// Failure-detection self-test: the scan's wait on a descriptor nothing
+// publishes must give up and flag it.
+__global__ void k_wait_probe(unsigned long long* desc, uint32_t* status) {
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    (void)await_descriptor(desc, status);
+}
+
 __global__ void __launch_bounds__(kThreads) k_scan(const int32_t* in, int32_t* out, int64_t n,
                                                    unsigned long long* desc, int32_t* ticket,
                                                    int32_t* total, uint32_t* status) {
@@ -263,19 +288,8 @@ __global__ void __launch_bounds__(kThreads) k_scan(const int32_t* in, int32_t* o
       while (!done) {
         const int idx = pred - lane;
         unsigned long long dsc = kFlagInclusive;  // lanes beyond block 0 contribute nothing
-        if (idx >= 0) {
-          int spins = 0;
-          dsc = peek(&desc[idx]);
-          while ((dsc >> 62) == 0) {
-            if (++spins > kSpinLimit) {
-              atomicOr(status, kStatusScanTimeout);
-              dsc = kFlagInclusive;
-              break;
-            }
-            __nanosleep(64);
-            dsc = peek(&desc[idx]);
-          }
-        }
+        if (idx >= 0)
+          dsc = await_descriptor(&desc[idx], status);
         const bool inclusive = (dsc >> 62) == 2 || idx < 0;
         const unsigned ballot = __ballot_sync(kFull, inclusive);
         const int first = ballot ? (__ffs(ballot) - 1) : 32;  // nearest inclusive predecessor
@@ -766,6 +780,11 @@ int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile
 void reset_launch_count() { t_launches = 0; }
 int64_t launch_count() { return t_launches; }
 void count_launches(int k) { t_launches += k; }
+
+cudaError_t launch_wait_probe(unsigned long long* desc, uint32_t* status, cudaStream_t st) {
+  k_wait_probe<<<1, 32, 0, st>>>(desc, status);
+  return cudaGetLastError();
+}
 
 // utils/detail/get_clusters.hpp:24-49 on the device: cluster -> points as CSR,
 // point ids ascending within a cluster (the order the reference's serial

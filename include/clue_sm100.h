@@ -158,6 +158,14 @@ clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t
  * inputs' contents may change between replays. Any other run replaces the
  * graph. Turning it off releases the graph. */
 clue_status clue_workspace_set_graphs(clue_workspace* ws, int32_t enable);
+/* Failure-detection self-test (no reference counterpart). Runs, on `device`,
+ * the bounded wait of the tile scan's decoupled look-back on a flag that
+ * nothing sets: the wait gives up after its limit (about 2^21 polls), the
+ * kernel records that in a status word and returns, and the call returns
+ * CLUE_ERR_TIMEOUT — the status every run reports when one of its waits gives
+ * up. The GPU stays usable afterwards. CLUE_ERR_RUNTIME means the wait did not
+ * report. Blocks until done. */
+clue_status clue_selftest_bounded_wait(int32_t device, void* stream);
 /* 1 when the workspace's last run was a graph replay, else 0. */
 clue_status clue_workspace_graph_replayed(const clue_workspace* ws, int32_t* replayed);
 /* Number of CUDA kernels the last run on this workspace enqueued (no reference
