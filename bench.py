@@ -449,6 +449,29 @@ def run_serving(args, local):
     return out
 
 
+def run_layered_3d(args):
+    """One layered 3-D event of 262,144 hits (lognormal energies, Gaussian kernel,
+    dc = 3, rhoc = 10, dm = 4): the largest 3-D event of the serving mix, whose
+    density keeps the reference's order. Two runs; profiles capture the second."""
+    import torch
+
+    import cluestering_b200 as clue
+    from cluestering_b200 import workloads as W
+    ev = W.layered_3d(262144, seed=11)
+    dev = torch.device("cuda", 0)
+    pts = clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev),
+                            outputs=("cluster_index",))
+    algo = clue.Clusterer(3.0, 10.0, 4.0)
+    for _ in range(2):
+        algo.make_clusters(pts, clue.EuclideanMetric(), clue.GaussianKernel(1.0, 1.0))
+    algo.set_profiling(True)
+    algo.make_clusters(pts, clue.EuclideanMetric(), clue.GaussianKernel(1.0, 1.0))
+    st = algo.stage_ms()
+    print(json.dumps({"case": "layered-3d", "points": ev.n, "n_clusters": algo.n_clusters(),
+                      "stage_ms": {k: round(v, 4) for k, v in st.items()}}), flush=True)
+    return 0
+
+
 def run_one_tile(args):
     """One event of 16,384 points uniform in [0, 10]^2 with a single tile (dc = 0.3): every
     density warp streams the same 16,384 candidates, which isolates the per-candidate cost
@@ -492,13 +515,16 @@ def main():
     ap.add_argument("--serve-stream", type=int, default=4000)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--skip-extras", action="store_true")
-    ap.add_argument("--case", choices=["one-tile"], default=None,
+    ap.add_argument("--case", choices=["one-tile", "layered-3d"], default=None,
                     help="profiling case instead of the benchmark: 'one-tile' clusters one "
                          "16,384-point event whose points all share one tile, so every warp of "
-                         "the density sweep streams the same box")
+                         "the density sweep streams the same box; 'layered-3d' clusters one "
+                         "262,144-hit layered 3-D event (the serving mix's heaviest kind)")
     args = ap.parse_args()
     if args.case == "one-tile":
         return run_one_tile(args)
+    if args.case == "layered-3d":
+        return run_layered_3d(args)
     if args.impl == "reference":
         # CPU arm: rank 0 times the CPU restatement; other ranks have no work.
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")),
