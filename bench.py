@@ -256,6 +256,7 @@ def run_ours(args, world, rank, local):
     e2e_ms = max_over_ranks(e2e_ms, world)
     e2e_value = R.job_throughput(points_all, e2e_ms)
     same = bool(np.array_equal(h.cluster_index, pts.cluster_index.cpu().numpy()))
+    pieces = algo_h.host_pieces()  # uploads and downloads overlap the clustering of other pieces
 
     extras = {}
     if rank == 0 and not args.skip_extras:
@@ -276,7 +277,8 @@ def run_ours(args, world, rank, local):
                        parallelism=f"replicas x{world} (events sharded by rank, no collective)"),
         "e2e": {"value": e2e_value, "unit": "points/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(ev.coords.nbytes + ev.weights.nbytes),
-                "d2h_bytes_per_step": int(n_total * 4), "matches_device_path": same},
+                "d2h_bytes_per_step": int(n_total * 4), "matches_device_path": same,
+                "pipelined_pieces": pieces},
         "gpu_launches": launches_per_run * args.steps,
         "n_clusters": n_clusters,
         "stage_ms": {k: round(v, 4) for k, v in stage.items()},

@@ -112,6 +112,7 @@ SIGNATURES = {
     "clue_workspace_set_graphs": (C.c_int, [_P, C.c_int32]),
     "clue_selftest_bounded_wait": (C.c_int, [C.c_int32, _P]),
     "clue_workspace_graph_replayed": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "clue_workspace_host_pieces": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "clue_tuning_defaults": (C.c_int, [C.POINTER(Tuning)]),
     "clue_workspace_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "clue_workspace_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),

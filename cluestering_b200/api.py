@@ -422,6 +422,12 @@ class Clusterer:
         L.check(L.load().clue_workspace_graph_replayed(self._workspace(), C.byref(r)))
         return bool(r.value)
 
+    def host_pieces(self) -> int:
+        """Pieces the last host-buffer run was pipelined in (1: one piece)."""
+        r = C.c_int32()
+        L.check(L.load().clue_workspace_host_pieces(self._workspace(), C.byref(r)))
+        return int(r.value)
+
     def set_profiling(self, enable: bool = True) -> None:
         L.check(L.load().clue_workspace_set_profiling(self._workspace(), int(enable)))
 

@@ -243,18 +243,24 @@ size_t scratch_bytes(const RunShape& s, bool sigma, bool unc, bool tags) {
   return place(&b, c, nullptr);
 }
 
-clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, bool unc, bool tags,
-                            int64_t staged) {
-  Capacity& c = ws->cap;
+// Whether the workspace's buffers already hold a run of this shape.
+bool capacity_fits(const clue_workspace* ws, const RunShape& s, bool sigma, bool unc, bool tags,
+                   int64_t staged) {
+  const Capacity& c = ws->cap;
   const int64_t scan_blocks = scan_blocks_for(std::max<int64_t>(s.n, s.n_tiles));
   const bool cells = s.D == 2 || s.D == 3;
-  const bool fits = c.points >= s.n && c.tiles >= s.n_tiles && c.events >= s.n_events &&
-                    c.chunks >= s.n_chunks && c.grids >= s.n_grids &&
-                    c.scan_blocks >= scan_blocks && c.dims >= s.D && (!sigma || c.sigma) &&
-                    (!unc || c.unc) && (!tags || c.tags) && (!cells || c.cells) &&
-                    c.staged_points >= staged;
-  if (fits)
+  return c.points >= s.n && c.tiles >= s.n_tiles && c.events >= s.n_events &&
+         c.chunks >= s.n_chunks && c.grids >= s.n_grids && c.scan_blocks >= scan_blocks &&
+         c.dims >= s.D && (!sigma || c.sigma) && (!unc || c.unc) && (!tags || c.tags) &&
+         (!cells || c.cells) && c.staged_points >= staged;
+}
+
+clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, bool unc, bool tags,
+                            int64_t staged) {
+  if (capacity_fits(ws, s, sigma, unc, tags, staged))
     return CLUE_OK;
+  const Capacity& c = ws->cap;
+  const bool cells = s.D == 2 || s.D == 3;
   // Grow every dimension that is short by 25 % headroom; keep what fits.
   auto grow = [](int64_t have, int64_t need) { return have >= need ? have : need + need / 4; };
   Capacity n = c;
@@ -532,7 +538,7 @@ clue_status upload_tables(clue_workspace* ws, const HostTables& t, cudaStream_t 
 // table building, no per-kernel launches, one graph launch.
 clue_status run_device(clue_workspace* ws, const clue_params* params, const clue_points* pts,
                        const uint32_t* sizes, int32_t n_events, int32_t grid_mode,
-                       cudaStream_t st, int64_t staged) {
+                       cudaStream_t st, int64_t staged, const Piece* piece) {
   clue_status s = check_params(params);
   if (s != CLUE_OK)
     return s;
@@ -541,7 +547,7 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   cudaError_t e = cudaSetDevice(ws->device);
   if (e != cudaSuccess)
     return fail_cuda(e, "cudaSetDevice");
-  const bool use_graph = ws->graphs && !ws->profiling && st != nullptr;
+  const bool use_graph = ws->graphs && !ws->profiling && st != nullptr && piece == nullptr;
   if (use_graph && graph_matches(ws, params, pts, sizes, n_events, grid_mode, staged)) {
     if ((e = cudaGraphLaunch(ws->graph_exec, st)) != cudaSuccess ||
         (e = cudaEventRecord(ws->staging_event, st)) != cudaSuccess)
@@ -552,25 +558,38 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
     return CLUE_OK;
   }
   ws->graph_replays_last = false;
-  HostTables t;
-  RunShape sh;
-  const char* err = nullptr;
-  if (!build_tables(pts->ndim, sizes, n_events, grid_mode, params->points_per_tile, &t, &sh, &err))
-    return fail(CLUE_ERR_INVALID_ARGUMENT, err);
-  if (sh.n != pts->n)
-    return fail(CLUE_ERR_INVALID_ARGUMENT, "the event sizes do not add up to the number of points");
-  bool any_sigma = false;
-  for (int d = 0; d < pts->ndim; ++d)
-    any_sigma |= pts->sigma[d] != nullptr;
-  if ((s = ensure_capacity(ws, sh, any_sigma, pts->density_uncertainty != nullptr,
-                           pts->tags != nullptr, staged)) != CLUE_OK)
-    return s;
-  if ((s = stage_tables(ws, t)) != CLUE_OK)
-    return s;
-  if (ws->graph_exec) {  // the cached graph reads the staging buffer just overwritten
-    if ((e = cudaGraphExecDestroy(ws->graph_exec)) != cudaSuccess)
-      return fail_cuda(e, "graph release");
-    ws->graph_exec = nullptr;
+  // A piece of a pipelined batch comes with its tables built, checked against
+  // the buffers and already on the device.
+  HostTables own_tables;
+  RunShape own_shape;
+  const HostTables& t = piece ? *piece->tables : own_tables;
+  const RunShape& sh = piece ? *piece->shape : own_shape;
+  DeviceBuffers b = ws->b;
+  if (piece) {
+    b.grids = piece->grids;
+    b.events = piece->events;
+    b.chunks = piece->chunks;
+  } else {
+    const char* err = nullptr;
+    if (!build_tables(pts->ndim, sizes, n_events, grid_mode, params->points_per_tile, &own_tables,
+                      &own_shape, &err))
+      return fail(CLUE_ERR_INVALID_ARGUMENT, err);
+    if (sh.n != pts->n)
+      return fail(CLUE_ERR_INVALID_ARGUMENT, "the event sizes do not add up to the number of points");
+    bool any_sigma = false;
+    for (int d = 0; d < pts->ndim; ++d)
+      any_sigma |= pts->sigma[d] != nullptr;
+    if ((s = ensure_capacity(ws, sh, any_sigma, pts->density_uncertainty != nullptr,
+                             pts->tags != nullptr, staged)) != CLUE_OK)
+      return s;
+    b = ws->b;
+    if ((s = stage_tables(ws, t)) != CLUE_OK)
+      return s;
+    if (ws->graph_exec) {  // the cached graph reads the staging buffer just overwritten
+      if ((e = cudaGraphExecDestroy(ws->graph_exec)) != cudaSuccess)
+        return fail_cuda(e, "graph release");
+      ws->graph_exec = nullptr;
+    }
   }
   // a failure of an earlier call whose status was not read would show up as
   // this run's launch error
@@ -588,17 +607,24 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   io.is_seed = pts->is_seed;
   io.rho = pts->rho;
   io.nh = pts->nearest_higher;
+  if (piece) {
+    io.piece_base = piece->base;
+    io.point_base = piece->point_base;
+    io.event_base = piece->event_base;
+  }
   const RunParams prm = make_run_params(params, pts, ws->tuning);
   reset_launch_count();
   if (use_graph && (e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return fail_cuda(e, "stream capture");
   // Everything from here to the end of the capture is stream work.
-  s = copy_tables(ws, t, st, !use_graph);
-  if (s == CLUE_OK && (e = launch_run(sh, prm, io, ws->b, st, ws->profiling ? ws->marks : nullptr)) !=
+  if (!piece)
+    s = copy_tables(ws, t, st, !use_graph);
+  if (s == CLUE_OK && (e = launch_run(sh, prm, io, b, st, ws->profiling ? ws->marks : nullptr)) !=
                           cudaSuccess)
     s = fail_cuda(e, "kernel launch");
-  // Seed count and status word come back with the run (read when needed).
-  if (s == CLUE_OK &&
+  // Seed count and status word come back with the run (read when needed); a
+  // pipelined batch reads them once, after its last piece.
+  if (s == CLUE_OK && !piece &&
       ((e = cudaMemcpyAsync(&ws->info->n_seeds, ws->b.counters + 1, sizeof(int32_t),
                             cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
        (e = cudaMemcpyAsync(&ws->info->status, ws->b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -652,62 +678,244 @@ clue_status wait_run(clue_workspace* ws) {
   return CLUE_OK;
 }
 
-// Copies one host point set into the workspace's staging buffers and points
-// `dev` at them.
+// Copies points [first, first + count) of a host point set into the
+// workspace's staging buffers, which are laid out for all h->n points, and
+// points `dev` at them (a point set of `count` points).
 clue_status stage_inputs(clue_workspace* ws, const clue_points* h, clue_points* dev,
-                         cudaStream_t st) {
+                         cudaStream_t st, int64_t first, int64_t count) {
   const int64_t n = h->n;
+  const int64_t o = first, m = count < 0 ? n - first : count;
   const int D = h->ndim;
   *dev = *h;
+  dev->n = m;
   cudaError_t e;
   for (int d = 0; d < D; ++d) {
-    float* dst = ws->b.in_coords + d * n;
-    if ((e = cudaMemcpyAsync(dst, h->coords[d], n * sizeof(float), cudaMemcpyHostToDevice, st)))
+    float* dst = ws->b.in_coords + d * n + o;
+    if ((e = cudaMemcpyAsync(dst, h->coords[d] + o, m * sizeof(float), cudaMemcpyHostToDevice, st)))
       return fail_cuda(e, "coordinate upload");
     dev->coords[d] = dst;
     if (h->sigma[d]) {
-      float* sd = ws->b.in_sigma + d * n;
-      if ((e = cudaMemcpyAsync(sd, h->sigma[d], n * sizeof(float), cudaMemcpyHostToDevice, st)))
+      float* sd = ws->b.in_sigma + d * n + o;
+      if ((e = cudaMemcpyAsync(sd, h->sigma[d] + o, m * sizeof(float), cudaMemcpyHostToDevice, st)))
         return fail_cuda(e, "sigma upload");
       dev->sigma[d] = sd;
     }
   }
-  if ((e = cudaMemcpyAsync(ws->b.in_weight, h->weight, n * sizeof(float), cudaMemcpyHostToDevice,
-                           st)))
+  if ((e = cudaMemcpyAsync(ws->b.in_weight + o, h->weight + o, m * sizeof(float),
+                           cudaMemcpyHostToDevice, st)))
     return fail_cuda(e, "weight upload");
-  dev->weight = ws->b.in_weight;
+  dev->weight = ws->b.in_weight + o;
   if (h->density_uncertainty) {
-    if ((e = cudaMemcpyAsync(ws->b.in_unc, h->density_uncertainty, n * sizeof(float),
+    if ((e = cudaMemcpyAsync(ws->b.in_unc + o, h->density_uncertainty + o, m * sizeof(float),
                              cudaMemcpyHostToDevice, st)))
       return fail_cuda(e, "uncertainty upload");
-    dev->density_uncertainty = ws->b.in_unc;
+    dev->density_uncertainty = ws->b.in_unc + o;
   }
   if (h->tags) {
-    if ((e = cudaMemcpyAsync(ws->b.in_tags, h->tags, n * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                             st)))
+    if ((e = cudaMemcpyAsync(ws->b.in_tags + o, h->tags + o, m * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, st)))
       return fail_cuda(e, "tag upload");
-    dev->tags = ws->b.in_tags;
+    dev->tags = ws->b.in_tags + o;
   }
-  dev->cluster_index = ws->b.out_cluster;
-  dev->is_seed = h->is_seed ? ws->b.out_seed : nullptr;
-  dev->rho = h->rho ? ws->b.out_rho : nullptr;
-  dev->nearest_higher = h->nearest_higher ? ws->b.out_nh : nullptr;
+  dev->cluster_index = ws->b.out_cluster + o;
+  dev->is_seed = h->is_seed ? ws->b.out_seed + o : nullptr;
+  dev->rho = h->rho ? ws->b.out_rho + o : nullptr;
+  dev->nearest_higher = h->nearest_higher ? ws->b.out_nh + o : nullptr;
   return CLUE_OK;
 }
 
-clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st) {
-  const size_t n = (size_t)h->n;
+// Copies the results of points [first, first + count) back to the host point set.
+clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st, int64_t first,
+                          int64_t count) {
+  const size_t o = (size_t)first, m = (size_t)(count < 0 ? h->n - first : count);
+  const auto down = [&](void* dst, const void* src) {
+    return cudaMemcpyAsync((char*)dst + 4 * o, (const char*)src + 4 * o, 4 * m,
+                           cudaMemcpyDeviceToHost, st);
+  };
   cudaError_t e;
-  if ((e = cudaMemcpyAsync(h->cluster_index, ws->b.out_cluster, n * 4, cudaMemcpyDeviceToHost, st)))
-    return fail_cuda(e, "result download");
-  if (h->is_seed && (e = cudaMemcpyAsync(h->is_seed, ws->b.out_seed, n * 4, cudaMemcpyDeviceToHost, st)))
-    return fail_cuda(e, "result download");
-  if (h->rho && (e = cudaMemcpyAsync(h->rho, ws->b.out_rho, n * 4, cudaMemcpyDeviceToHost, st)))
-    return fail_cuda(e, "result download");
-  if (h->nearest_higher &&
-      (e = cudaMemcpyAsync(h->nearest_higher, ws->b.out_nh, n * 4, cudaMemcpyDeviceToHost, st)))
+  if ((e = down(h->cluster_index, ws->b.out_cluster)) ||
+      (h->is_seed && (e = down(h->is_seed, ws->b.out_seed))) ||
+      (h->rho && (e = down(h->rho, ws->b.out_rho))) ||
+      (h->nearest_higher && (e = down(h->nearest_higher, ws->b.out_nh))))
     return fail_cuda(e, "result download");
   return CLUE_OK;
+}
+
+namespace {
+
+// Host batches of at least kPieceMinPoints points with one grid per event run
+// as up to kMaxPieces pieces of whole events, so that the upload of a piece
+// overlaps the clustering of the one before it and its download the clustering
+// of the one after. Events are independent under per-event grids, so a piece's
+// results are those of the whole batch; the pieces only renumber (Piece).
+constexpr int64_t kPieceMinPoints = int64_t(1) << 22;
+constexpr int kMaxPieces = 4;
+
+// Event boundaries of the pieces: cuts[p] .. cuts[p + 1], about equal in points.
+std::vector<int32_t> piece_cuts(const uint32_t* sizes, int32_t n_events, int64_t n) {
+  const int64_t k = std::min<int64_t>({kMaxPieces, n / kPieceMinPoints, n_events});
+  std::vector<int32_t> cuts{0};
+  int64_t acc = 0;
+  for (int32_t e = 0; e < n_events; ++e) {
+    acc += sizes[e];
+    const int64_t p = (int64_t)cuts.size();  // the cut after this event would end piece p - 1
+    if (p < k && e + 1 < n_events && acc * k >= p * n)
+      cuts.push_back(e + 1);
+  }
+  cuts.push_back(n_events);
+  return cuts;
+}
+
+}  // namespace
+
+clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const clue_points* h,
+                            const uint32_t* sizes, cudaStream_t st, const HostTables& whole,
+                            const HostTables& all, const std::vector<int32_t>& cuts,
+                            const std::vector<Piece>& pieces);
+
+// The pipelined form of run_host (see kPieceMinPoints). Returns false, having
+// enqueued nothing, when the batch does not split; else the call's status is
+// in *out.
+bool run_host_pieces(clue_workspace* ws, const clue_params* params, const clue_points* h,
+                     const uint32_t* sizes, int32_t n_events, cudaStream_t st,
+                     const HostTables& whole, bool any_sigma, clue_status* out) {
+  const std::vector<int32_t> cuts = piece_cuts(sizes, n_events, h->n);
+  const int P = (int)cuts.size() - 1;
+  if (P < 2)
+    return false;
+  // Each piece's tables, and all of them end to end: piece p runs on its slice
+  // of the table buffers, so one upload ahead of the points serves every piece.
+  std::vector<HostTables> tabs(P);
+  std::vector<RunShape> shapes(P);
+  std::vector<int64_t> first(P + 1, 0);
+  HostTables all;
+  std::vector<size_t> grid_at(P), event_at(P), chunk_at(P);
+  for (int p = 0; p < P; ++p) {
+    const char* err = nullptr;
+    if (!build_tables(h->ndim, sizes + cuts[p], cuts[p + 1] - cuts[p], CLUE_GRID_PER_EVENT,
+                      params->points_per_tile, &tabs[p], &shapes[p], &err))
+      return false;
+    first[p + 1] = first[p] + shapes[p].n;
+    // every piece must fit the buffers sized for the whole batch: nothing may
+    // be reallocated under the uploads in flight
+    if (!capacity_fits(ws, shapes[p], any_sigma, h->density_uncertainty != nullptr,
+                       h->tags != nullptr, h->n))
+      return false;
+    grid_at[p] = all.grids.size();
+    event_at[p] = all.events.size();
+    chunk_at[p] = all.chunks.size();
+    all.grids.insert(all.grids.end(), tabs[p].grids.begin(), tabs[p].grids.end());
+    all.events.insert(all.events.end(), tabs[p].events.begin(), tabs[p].events.end());
+    all.chunks.insert(all.chunks.end(), tabs[p].chunks.begin(), tabs[p].chunks.end());
+  }
+  if ((int64_t)all.grids.size() > ws->cap.grids || (int64_t)all.events.size() > ws->cap.events ||
+      (int64_t)all.chunks.size() > ws->cap.chunks)
+    return false;
+  std::vector<Piece> pieces(P);
+  for (int p = 0; p < P; ++p) {
+    Piece& q = pieces[p];
+    q.base = ws->b.counters + 8;
+    q.point_base = first[p];
+    q.event_base = cuts[p];
+    q.tables = &tabs[p];
+    q.shape = &shapes[p];
+    q.grids = ws->b.grids + grid_at[p];
+    q.events = ws->b.events + event_at[p];
+    q.chunks = ws->b.chunks + chunk_at[p];
+  }
+  *out = pipeline_pieces(ws, params, h, sizes, st, whole, all, cuts, pieces);
+  return true;
+}
+
+// Stream order: [tables] on st, then the point uploads of every piece on `up`;
+// piece p clusters on st once its upload is in, and its results go back on
+// `down` once it is clustered, while the next piece clusters.
+clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const clue_points* h,
+                            const uint32_t* sizes, cudaStream_t st, const HostTables& whole,
+                            const HostTables& all, const std::vector<int32_t>& cuts,
+                            const std::vector<Piece>& pieces) {
+  const int P = (int)pieces.size();
+  cudaError_t e;
+  if (!ws->up && (e = cudaStreamCreateWithFlags(&ws->up, cudaStreamNonBlocking)))
+    return fail_cuda(e, "upload stream");
+  if (!ws->down && (e = cudaStreamCreateWithFlags(&ws->down, cudaStreamNonBlocking)))
+    return fail_cuda(e, "download stream");
+  // events: [0] tables up, [1] downloads done, then per piece uploaded and clustered
+  const size_t n_ev = 2 + 2 * (size_t)kMaxPieces;
+  while (ws->piece_events.size() < n_ev) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)))
+      return fail_cuda(e, "piece event");
+    ws->piece_events.push_back(ev);
+  }
+  cudaEvent_t* ev = ws->piece_events.data();
+  cudaEvent_t *uploaded = ev + 2, *clustered = ev + 2 + kMaxPieces;
+  clue_status s = stage_tables(ws, all);
+  if (s != CLUE_OK)
+    return s;
+  if (ws->graph_exec) {  // the cached graph reads the staging buffer just overwritten
+    if ((e = cudaGraphExecDestroy(ws->graph_exec)) != cudaSuccess)
+      return fail_cuda(e, "graph release");
+    ws->graph_exec = nullptr;
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return fail_cuda(e, "a CUDA error left pending before this run");
+  if ((s = copy_tables(ws, all, st, true)) != CLUE_OK)
+    return s;
+  if ((e = cudaEventRecord(ev[0], st)) || (e = cudaStreamWaitEvent(ws->up, ev[0], 0)))
+    return fail_cuda(e, "piece ordering");
+  // From here on work is in flight on `up`: every return first waits for it.
+  const auto settle = [&](clue_status r) {
+    cudaStreamSynchronize(ws->up);
+    cudaStreamSynchronize(ws->down);
+    return r;
+  };
+  std::vector<clue_points> dev(P);
+  for (int p = 0; p < P && s == CLUE_OK; ++p) {
+    s = stage_inputs(ws, h, &dev[p], ws->up, pieces[p].point_base, pieces[p].shape->n);
+    if (s == CLUE_OK && (e = cudaEventRecord(uploaded[p], ws->up)))
+      s = fail_cuda(e, "piece ordering");
+  }
+  int32_t* base = pieces[0].base;
+  if (s == CLUE_OK && (e = launch_fill32(base, 1, 0, st)))
+    s = fail_cuda(e, "piece base");
+  int64_t launches = 1;
+  for (int p = 0; p < P && s == CLUE_OK; ++p) {
+    if ((e = cudaStreamWaitEvent(st, uploaded[p], 0))) {
+      s = fail_cuda(e, "piece ordering");
+      break;
+    }
+    s = run_device(ws, params, &dev[p], sizes + cuts[p], cuts[p + 1] - cuts[p], CLUE_GRID_PER_EVENT,
+                   st, h->n, &pieces[p]);
+    launches += ws->last_launches;
+    if (s == CLUE_OK && (e = cudaEventRecord(clustered[p], st)))
+      s = fail_cuda(e, "piece ordering");
+  }
+  for (int p = 0; p < P && s == CLUE_OK; ++p) {
+    if ((e = cudaStreamWaitEvent(ws->down, clustered[p], 0)))
+      s = fail_cuda(e, "piece ordering");
+    else
+      s = fetch_outputs(ws, h, ws->down, pieces[p].point_base, pieces[p].shape->n);
+  }
+  if (s == CLUE_OK && ((e = cudaEventRecord(ev[1], ws->down)) || (e = cudaStreamWaitEvent(st, ev[1], 0))))
+    s = fail_cuda(e, "piece ordering");
+  // the batch's cluster count is where the last piece left the base
+  if (s == CLUE_OK &&
+      ((e = cudaMemcpyAsync(&ws->info->n_seeds, base, sizeof(int32_t), cudaMemcpyDeviceToHost, st)) ||
+       (e = cudaMemcpyAsync(&ws->info->status, ws->b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            st))))
+    s = fail_cuda(e, "result copy");
+  if (s != CLUE_OK)
+    return settle(s);
+  cudaEventRecord(ws->run_event, st);
+  ws->last_n = h->n;
+  ws->last_events = whole.events;
+  ws->last_labels = ws->b.out_cluster;
+  ws->last_launches = launches;
+  ws->last_pieces = P;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return settle(fail_cuda(e, "stream synchronize"));
+  return wait_run(ws);
 }
 
 clue_status run_host(clue_workspace* ws, const clue_params* params, const clue_points* h,
@@ -734,6 +942,12 @@ clue_status run_host(clue_workspace* ws, const clue_params* params, const clue_p
   if ((s = ensure_capacity(ws, sh, any_sigma, h->density_uncertainty != nullptr, h->tags != nullptr,
                            h->n)) != CLUE_OK)
     return s;
+  if (grid_mode == CLUE_GRID_PER_EVENT && n_events > 1 && h->n >= 2 * kPieceMinPoints &&
+      !ws->profiling) {
+    if (run_host_pieces(ws, params, h, sizes, n_events, st, t, any_sigma, &s))
+      return s;
+  }
+  ws->last_pieces = 1;
   clue_points dev;
   if ((s = stage_inputs(ws, h, &dev, st)) != CLUE_OK)
     return s;
@@ -820,6 +1034,13 @@ clue_status clue_workspace_destroy(clue_workspace* ws) {
       cudaEventDestroy(m);
   if (ws->graph_exec)
     cudaGraphExecDestroy(ws->graph_exec);
+  for (cudaStream_t s : {ws->up, ws->down})
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  for (cudaEvent_t ev : ws->piece_events)
+    cudaEventDestroy(ev);
   delete ws;
   return CLUE_OK;
 }
@@ -892,6 +1113,13 @@ clue_status clue_workspace_graph_replayed(const clue_workspace* ws, int32_t* rep
   if (!ws || !replayed)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
   *replayed = ws->graph_replays_last ? 1 : 0;
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_host_pieces(const clue_workspace* ws, int32_t* pieces) {
+  if (!ws || !pieces)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  *pieces = ws->last_pieces;
   return CLUE_OK;
 }
 

@@ -47,6 +47,11 @@ struct clue_workspace {
     std::vector<uint32_t> sizes;
   } graph_key{};
   bool graph_replays_last = false;  // whether the last run was a replay
+  // Pipelined host batches: uploads run on `up`, downloads on `down`, both
+  // ordered against the caller's stream by these events (created on first use).
+  cudaStream_t up = nullptr, down = nullptr;
+  std::vector<cudaEvent_t> piece_events;
+  int32_t last_pieces = 0;  // pieces of the last host run (1: not pipelined)
 };
 
 namespace clue_impl {
@@ -57,14 +62,30 @@ clue_status check_params(const clue_params* p);
 clue_status check_points(const clue_points* pts, bool need_output, int metric_kind);
 clue_status ensure_capacity(clue_workspace* ws, const RunShape& s, bool sigma, bool unc, bool tags,
                             int64_t staged);
+// One piece of a pipelined batch: where its cluster ids start (a device
+// counter the piece advances), its first point and event in the batch, and
+// its tables, built on the host and already copied to the device.
+struct Piece {
+  int32_t* base = nullptr;
+  int64_t point_base = 0;
+  int32_t event_base = 0;
+  const HostTables* tables = nullptr;
+  const RunShape* shape = nullptr;
+  GridDesc* grids = nullptr;
+  EventDesc* events = nullptr;
+  Chunk* chunks = nullptr;
+};
 clue_status run_device(clue_workspace* ws, const clue_params* params, const clue_points* pts,
                        const uint32_t* sizes, int32_t n_events, int32_t grid_mode,
-                       cudaStream_t st, int64_t staged);
+                       cudaStream_t st, int64_t staged, const Piece* piece = nullptr);
 clue_status run_host(clue_workspace* ws, const clue_params* params, const clue_points* h,
                      const uint32_t* sizes, int32_t n_events, int32_t grid_mode, cudaStream_t st);
+// Stage points [first, first + count) of `h` (count < 0: all of them) in the
+// workspace's input buffers, which are laid out for all h->n points.
 clue_status stage_inputs(clue_workspace* ws, const clue_points* h, clue_points* dev,
-                         cudaStream_t st);
-clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st);
+                         cudaStream_t st, int64_t first = 0, int64_t count = -1);
+clue_status fetch_outputs(clue_workspace* ws, const clue_points* h, cudaStream_t st,
+                          int64_t first = 0, int64_t count = -1);
 clue_status wait_run(clue_workspace* ws);
 float sqrt_threshold(float r);
 clue_tuning default_tuning();

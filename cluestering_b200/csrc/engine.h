@@ -107,6 +107,14 @@ struct RunIO {
   int32_t* is_seed = nullptr;
   float* rho = nullptr;
   int32_t* nh = nullptr;
+  // A run over one piece of a larger batch (events [event_base, ...), points
+  // [point_base, ...)): its cluster ids and seed slots start at *piece_base,
+  // which the run then advances by its seed count; seed indices and
+  // nearest-higher indices count from point_base, seed events from
+  // event_base. Null for a run that is the whole batch.
+  int32_t* piece_base = nullptr;
+  int64_t point_base = 0;
+  int32_t event_base = 0;
 };
 
 // Host tables built for a run.
@@ -132,12 +140,14 @@ cudaError_t launch_run(const RunShape& shape, const RunParams& prm, const RunIO&
                        const DeviceBuffers& b, cudaStream_t stream,
                        cudaEvent_t* marks = nullptr);
 
-// Turns the batch-wide results of a run into per-event results: cluster ids
-// restart at 0 in every event and nearest-higher ids become event-local, which
-// is exactly what each event gets when clustered alone.
 // Runs the tile scan's bounded wait on `desc` (zeroed: nothing publishes it);
 // the kernel sets a bit in `status` when the wait gives up.
 cudaError_t launch_wait_probe(unsigned long long* desc, uint32_t* status, cudaStream_t stream);
+// Sets `words` 32-bit words at p to `value` with a kernel (no copy engine).
+cudaError_t launch_fill32(void* p, int64_t words, uint32_t value, cudaStream_t stream);
+// Turns the batch-wide results of a run into per-event results: cluster ids
+// restart at 0 in every event and nearest-higher ids become event-local, which
+// is exactly what each event gets when clustered alone.
 cudaError_t launch_localize(const DeviceBuffers& b, int32_t n_events, int64_t n,
                             int32_t* cluster_index, int32_t* nh, cudaStream_t stream);
 

@@ -224,6 +224,29 @@ __global__ void k_wait_probe(unsigned long long* desc, uint32_t* status) {
     (void)await_descriptor(desc, status);
 }
 
+// Clears and copies of a run are kernels rather than cudaMemsetAsync /
+// cudaMemcpyAsync: a run then never waits in a copy engine's queue behind the
+// point uploads of a pipelined host batch.
+__global__ void k_fill32(uint32_t* p, int64_t n, uint32_t v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void k_copy32(uint32_t* dst, const uint32_t* src, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+// Zeroes the scan's look-back descriptors and its block ticket.
+__global__ void k_scan_reset(unsigned long long* desc, int blocks, int32_t* ticket) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < blocks; i += gridDim.x * blockDim.x)
+    desc[i] = 0ull;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    *ticket = 0;
+}
+
 __global__ void __launch_bounds__(kThreads) k_scan(const int32_t* in, int32_t* out, int64_t n,
                                                    unsigned long long* desc, int32_t* ticket,
                                                    int32_t* total, uint32_t* status) {
@@ -678,10 +701,15 @@ __global__ void k_jump(int64_t n, int32_t* parent) {
 // itself): a chain runs between neighbouring points, so its steps stay within
 // a few tiles and mostly hit cache, and the lanes of a warp, which start on
 // neighbouring points, share most of their chains.
+// A piece of a larger batch (piece_base set) numbers its clusters and seed
+// slots from *piece_base and its seed and nearest-higher indices from
+// point_base.
 __global__ void k_labels(int64_t n, int32_t* parent, const int32_t* perm, const int32_t* seed_flag,
                          const int32_t* seed_rank, const int32_t* point_event,
                          int32_t* cluster_index, int32_t* seeds, int32_t* seed_event,
-                         uint32_t* status) {
+                         uint32_t* status, const int32_t* piece_base, int32_t point_base,
+                         int32_t event_base, int32_t* nh) {
+  const int32_t base = piece_base ? *piece_base : 0;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (int64_t)gridDim.x * blockDim.x) {
     int x = (int)s;
@@ -701,12 +729,20 @@ __global__ void k_labels(int64_t n, int32_t* parent, const int32_t* perm, const 
     }
     const int gi = perm[s];
     const int gr = perm[x];
-    cluster_index[gi] = seed_flag[gr] ? seed_rank[gr] : -1;
+    cluster_index[gi] = seed_flag[gr] ? seed_rank[gr] + base : -1;
     if (seed_flag[gi]) {
-      seeds[seed_rank[gi]] = gi;
-      seed_event[seed_rank[gi]] = point_event[gi];
+      seeds[seed_rank[gi] + base] = gi + point_base;
+      seed_event[seed_rank[gi] + base] = point_event[gi] + event_base;
     }
+    if (nh && nh[gi] >= 0)
+      nh[gi] += point_base;
   }
+}
+
+// Moves a piece's base past its seeds, for the next piece of the batch.
+__global__ void k_advance_piece(int32_t* piece_base, const int32_t* n_seeds) {
+  if (threadIdx.x == 0)
+    *piece_base += *n_seeds;
 }
 
 // Per-event relabelling after a batched run with one grid per event.
@@ -729,19 +765,23 @@ int grid_for(int64_t n, int per_block = kThreads) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
 }
 
+cudaError_t fill32(void* p, int64_t words, uint32_t v, cudaStream_t st) {
+  if (words <= 0)
+    return cudaSuccess;
+  k_fill32<<<grid_for(words), kThreads, 0, st>>>((uint32_t*)p, words, v);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
                  const DeviceBuffers& b, cudaStream_t st) {
-  const int blocks = scan_blocks_for(n);
-  cudaError_t e = cudaMemsetAsync(b.scan_desc, 0, sizeof(unsigned long long) * blocks, st);
-  if (e != cudaSuccess)
-    return e;
-  e = cudaMemsetAsync(b.counters, 0, sizeof(int32_t), st);  // ticket
-  if (e != cudaSuccess)
-    return e;
   if (n == 0)
-    return cudaMemsetAsync(total, 0, sizeof(int32_t), st);
+    return fill32(total, 1, 0, st);
+  const int blocks = scan_blocks_for(n);
+  k_scan_reset<<<(blocks + kThreads - 1) / kThreads, kThreads, 0, st>>>(b.scan_desc, blocks,
+                                                                        b.counters);  // [0]: ticket
   k_scan<<<blocks, kThreads, 0, st>>>(in, out, n, b.scan_desc, b.counters, total, b.status);
-  count_launches(1);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -752,7 +792,7 @@ cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* i
                           const DeviceBuffers& b, cudaStream_t st, const int32_t* event_exact = nullptr) {
   int32_t* oversize_count = b.counters + 2;
   int32_t* large_count = b.counters + 3;
-  cudaError_t e = cudaMemsetAsync(oversize_count, 0, 2 * sizeof(int32_t), st);
+  cudaError_t e = fill32(oversize_count, 2, 0, st);  // and large_count, the next counter
   if (e != cudaSuccess)
     return e;
   const int64_t warps_per_block = kThreads / 32;
@@ -780,6 +820,10 @@ int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile
 void reset_launch_count() { t_launches = 0; }
 int64_t launch_count() { return t_launches; }
 void count_launches(int k) { t_launches += k; }
+
+cudaError_t launch_fill32(void* p, int64_t words, uint32_t value, cudaStream_t st) {
+  return fill32(p, words, value, st);
+}
 
 cudaError_t launch_wait_probe(unsigned long long* desc, uint32_t* status, cudaStream_t st) {
   k_wait_probe<<<1, 32, 0, st>>>(desc, status);
@@ -867,13 +911,14 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // counting sort by tile
   CLUE_MARK(1);
-  CLUE_CHECK(cudaMemsetAsync(b.tile_count, 0, sizeof(int32_t) * sh.n_tiles, st));
+  CLUE_CHECK(fill32(b.tile_count, sh.n_tiles, 0, st));
   k_bin<<<sh.n_chunks, kThreads, 0, st>>>(prm, x, b.chunks, b.events, b.grids, b.tile_of,
                                            b.point_event, b.tile_count, io.weight, exact);
   CLUE_LAUNCHED();
   CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));
-  CLUE_CHECK(cudaMemcpyAsync(b.tile_cursor, b.tile_offset, sizeof(int32_t) * sh.n_tiles,
-                             cudaMemcpyDeviceToDevice, st));
+  k_copy32<<<grid_for(sh.n_tiles), kThreads, 0, st>>>((uint32_t*)b.tile_cursor,
+                                                     (const uint32_t*)b.tile_offset, sh.n_tiles);
+  CLUE_LAUNCHED();
   k_scatter<<<grid_for(n), kThreads, 0, st>>>(b.tile_of, n, b.tile_cursor, b.perm);
   CLUE_LAUNCHED();
   // Exact-sum events need no ascending order within their tiles when nothing
@@ -950,10 +995,17 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     k_jump<<<grid_for(n), kThreads, 0, st>>>(n, b.parent);
     CLUE_LAUNCHED();
   }
+  const bool piece = io.piece_base != nullptr;
   k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.perm, b.seed_flag, b.seed_rank,
                                              b.point_event, io.cluster_index, b.seeds,
-                                             b.seed_event, b.status);
+                                             b.seed_event, b.status, io.piece_base,
+                                             (int32_t)io.point_base, io.event_base,
+                                             piece && io.point_base ? io.nh : nullptr);
   CLUE_LAUNCHED();
+  if (piece) {
+    k_advance_piece<<<1, 32, 0, st>>>(io.piece_base, b.counters + 1);
+    CLUE_LAUNCHED();
+  }
   CLUE_MARK(6);
 #undef CLUE_MARK
 #undef CLUE_LAUNCHED

@@ -168,6 +168,11 @@ clue_status clue_workspace_set_graphs(clue_workspace* ws, int32_t enable);
 clue_status clue_selftest_bounded_wait(int32_t device, void* stream);
 /* 1 when the workspace's last run was a graph replay, else 0. */
 clue_status clue_workspace_graph_replayed(const clue_workspace* ws, int32_t* replayed);
+/* Pieces the last host-buffer run on this workspace was split into: a batch of
+ * at least 2^23 points with one grid per event runs as up to 4 pieces of whole
+ * events, so that host<->device copies overlap the clustering; 1 otherwise.
+ * Results are the same either way. */
+clue_status clue_workspace_host_pieces(const clue_workspace* ws, int32_t* pieces);
 /* Number of CUDA kernels the last run on this workspace enqueued (no reference
  * counterpart; a check that the run executed on the GPU). */
 clue_status clue_workspace_kernel_launches(const clue_workspace* ws, int64_t* launches);

@@ -374,6 +374,61 @@ def test_host_and_device_entry_points_agree():
     assert same_partition(a["ci"], b["ci"])
 
 
+def _pipelined_against_device(ev, sizes, prm, kernel):
+    import torch
+    n = ev.n
+    h = clue.PointsHost(ev.coords, ev.weights)
+    h.is_seed = np.zeros(n, np.int32)
+    h.rho = np.zeros(n, np.float32)
+    h.nearest_higher = np.zeros(n, np.int32)
+    ch = clue.Clusterer(*prm)
+    ch.make_clusters(h, clue.EuclideanMetric(), kernel, batch_item_sizes=sizes,
+                     grid_mode=clue.GRID_PER_EVENT)
+    dev = torch.device("cuda", 0)
+    d = clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev),
+                          outputs=("cluster_index", "is_seed", "rho", "nearest_higher"))
+    cd = clue.Clusterer(*prm)
+    cd.make_clusters(d, clue.EuclideanMetric(), kernel, batch_item_sizes=sizes,
+                     grid_mode=clue.GRID_PER_EVENT)
+    assert np.array_equal(h.cluster_index, d.cluster_index.cpu().numpy())
+    assert np.array_equal(h.is_seed, d.is_seed.cpu().numpy())
+    assert np.array_equal(h.rho.view(np.int32), d.rho.cpu().numpy().view(np.int32))
+    assert np.array_equal(h.nearest_higher, d.nearest_higher.cpu().numpy())
+    assert ch.n_clusters() == cd.n_clusters()
+    assert np.array_equal(ch.getSeeds(), cd.getSeeds())
+    oh, kh = ch.getSampleAssociations()
+    od, kd = cd.getSampleAssociations()
+    assert kh == kd and np.array_equal(oh, od)
+    for a, b in zip(ch.getClustersDevice(), cd.getClustersDevice()):
+        assert torch.equal(a, b)
+    return ch.host_pieces()
+
+
+def test_pipelined_host_batch_equals_the_device_batch():
+    # 2^23 points or more with one grid per event: the host entry point runs the
+    # batch in pieces of whole events; ids, seeds and nearest-higher indices keep
+    # their whole-batch numbering
+    ev, sizes = W.batch_2d(640, 4096, 32768, seed=61)
+    assert ev.n >= 1 << 23
+    assert _pipelined_against_device(ev, sizes, (1.5, 5.0, 1.5), clue.FlatKernel(0.5)) >= 2
+
+
+def test_pipelined_host_batch_equals_the_device_batch_3d_gaussian():
+    evs = [W.layered_3d(int(m), seed=70 + i) for i, m in
+           enumerate(W.log_uniform_sizes(160, 16384, 131072, seed=71))]
+    sizes = np.array([e.n for e in evs], np.uint32)
+    ev = W.Event(np.ascontiguousarray(np.concatenate([e.coords for e in evs], axis=1)),
+                 np.concatenate([e.weights for e in evs]))
+    if ev.n < 1 << 23:
+        pytest.skip("the 3-D batch came out below the pipelining size")
+    assert _pipelined_against_device(ev, sizes, (3.0, 10.0, 4.0), clue.GaussianKernel(1.0, 1.0)) >= 2
+
+
+def test_small_host_batch_runs_in_one_piece():
+    ev, sizes = W.batch_2d(16, 256, 4096, seed=62)
+    assert _pipelined_against_device(ev, sizes, (1.5, 5.0, 1.5), clue.FlatKernel(0.5)) == 1
+
+
 # ---- launch tuning: results must not depend on it ---------------------------------------------
 
 TUNINGS = [
