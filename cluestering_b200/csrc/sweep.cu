@@ -430,7 +430,7 @@ __device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const Gri
 
 constexpr int kCellTarget = 2;     // average points per cell
 constexpr int kCellSlots = 2048;   // cells per tile at most (45^2, 12^3)
-constexpr int kCellWarps = 4;      // warps per block of k_cells
+constexpr int kCellWarps = 8;      // warps per block of k_cells
 
 template <int D>
 __host__ __device__ constexpr int cell_dim_max() {
@@ -1478,23 +1478,25 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
   }
 }
 
-// Cell layouts of all tiles. Blocks [0, warp_blocks) give one warp to each
-// tile of at most kLargeTilePoints points; the other blocks take the larger
-// tiles, which the tile sort listed, one block each, so a dense tile of
-// thousands of points does not hold up the launch on one warp.
+// Cell layouts of all tiles. Blocks [0, large_blocks) take the tiles of more
+// than kLargeTilePoints points, which the tile sort listed, one block each, so
+// a dense tile of thousands of points does not hold up the launch on one warp;
+// they come first so that the heaviest tiles do not run as a tail. The other
+// blocks give one warp to each smaller tile.
 constexpr int kWarpCellSlots = kLargeTilePoints / kCellTarget;  // s^D * 2 <= m <= 256
 template <int D>
 __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a,
-                                                          int warp_blocks) {
+                                                          int large_blocks) {
   constexpr int E = box_classes<D>();
   static_assert(kWarpCellSlots * kCellWarps <= kCellSlots, "warp counters fit the block's");
   __shared__ int s_cnt[kCellSlots];
   __shared__ int s_cnt2[kCellSlots];
   __shared__ int s_cls[kCellWarps][E];
   const int warp = threadIdx.x >> 5;
-  if ((int)blockIdx.x < warp_blocks) {
-    const int64_t stride = (int64_t)warp_blocks * kCellWarps;
-    for (int64_t t = (int64_t)blockIdx.x * kCellWarps + warp; t < a.n_tiles; t += stride) {
+  if ((int)blockIdx.x >= large_blocks) {
+    const int64_t wb = (int64_t)blockIdx.x - large_blocks;
+    const int64_t stride = ((int64_t)gridDim.x - large_blocks) * kCellWarps;
+    for (int64_t t = wb * kCellWarps + warp; t < a.n_tiles; t += stride) {
       if (a.tile_offset[t + 1] - a.tile_offset[t] > kLargeTilePoints)
         continue;
       tile_cells<D, 32>(p, a, t, s_cnt + warp * kWarpCellSlots, s_cls[warp],
@@ -1502,7 +1504,7 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
     }
   } else {
     const int n_large = *a.large_count;
-    for (int k = (int)blockIdx.x - warp_blocks; k < n_large; k += (int)gridDim.x - warp_blocks)
+    for (int k = (int)blockIdx.x; k < n_large; k += large_blocks)
       tile_cells<D, kCellWarps * 32>(p, a, a.large_tiles[k], s_cnt, s_cls[0], s_cnt2);
   }
 }
@@ -1521,6 +1523,7 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
   if (lb2 > eff2 || lb2 >= st.hi)
     return;
   const float4* __restrict__ rec = a.rec_nh;
+#pragma unroll 4
   for (int q = ci.start; q < ci.end; ++q) {
     const float4 r = __ldg(&rec[q]);
     const uint32_t tag_j = D == 2 ? __float_as_uint(r.w) : __ldg(&a.rec_tag[q]);
@@ -1538,8 +1541,13 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
 // within the current bound. The result is the eligible candidate of least
 // distance, ties to the larger key (ClusteringKernels.hpp:195-202), as in
 // k_nearest_higher_fast, over exactly the same candidates.
+// The search is bound by the latency of its dependent loads (cell info, box,
+// members), so the 2-D form trades registers for resident warps: 8 blocks of
+// 256 threads per SM measured 8.3 ms on the 46.5 M-point batch against 9.4 ms
+// at 5 and 10.8 ms at 4, small spills included. The 3-D form, with more state
+// per lane, stays at 4.
 template <int D>
-__global__ void __launch_bounds__(kThreads, 4) k_nearest_higher_cells(const RunParams p,
+__global__ void __launch_bounds__(kThreads, D == 2 ? 8 : 4) k_nearest_higher_cells(const RunParams p,
                                                                    const SweepArgs a) {
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_nh;
@@ -1700,11 +1708,11 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
         (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, 148 * 32));
     // blocks for the large tiles: at most one per tile that can be large
     const int large_blocks =
-        (int)std::max<int64_t>(1, std::min<int64_t>(a.n / (kLargeTilePoints + 1), 148 * 4));
+        (int)std::max<int64_t>(1, std::min<int64_t>(a.n / (kLargeTilePoints + 1), 148 * 24));
     if (D == 2)
-      k_cells<2><<<warp_blocks + large_blocks, kCellWarps * 32, 0, st>>>(p, a, warp_blocks);
+      k_cells<2><<<large_blocks + warp_blocks, kCellWarps * 32, 0, st>>>(p, a, large_blocks);
     else
-      k_cells<3><<<warp_blocks + large_blocks, kCellWarps * 32, 0, st>>>(p, a, warp_blocks);
+      k_cells<3><<<large_blocks + warp_blocks, kCellWarps * 32, 0, st>>>(p, a, large_blocks);
     count_launches(1);
   }
   return cudaGetLastError();
