@@ -48,10 +48,11 @@ CONFIG = {
 # index and writes nh (4D + 12); the whole pipeline moves 20D + 64.
 BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4 * D + 12,
                    "pipeline": lambda D: 20 * D + 64}
-# DRAM bytes (read + write) per point of each sweep, from one ncu capture of the
-# 1,024-event batch (profiles/sweeps_batch_2d_1024ev.md: 922.5 MB and 651.8 MB
-# for 10,621,973 points); a launch's traffic grows with the points it processes.
-DRAM_BYTES_PER_POINT = {"density": 86.9, "nearest_higher": 61.4}
+# DRAM bytes (read + write) per point of each sweep, from ncu captures of the
+# 1,024-event batch (profiles/sweeps_batch_2d_1024ev.md: 922.5 MB for density;
+# profiles/nearest_higher_and_cells_batch_2d_1024ev.md: 703.2 MB for nearest
+# higher; 10,621,973 points); a launch's traffic grows with the points it processes.
+DRAM_BYTES_PER_POINT = {"density": 86.9, "nearest_higher": 66.2}
 
 
 def measured_peaks():
