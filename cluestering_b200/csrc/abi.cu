@@ -751,15 +751,23 @@ namespace {
 constexpr int64_t kPieceMinPoints = int64_t(1) << 22;
 constexpr int kMaxPieces = 4;
 
-// Event boundaries of the pieces: cuts[p] .. cuts[p + 1], about equal in points.
+// Event boundaries of the pieces: cuts[p] .. cuts[p + 1]. Piece p holds about
+// min(p + 1, 3) shares of the points (1:2:3:3 for four pieces): the first
+// piece is small, so clustering starts after a short upload, and each later
+// piece uploads (about 2.6 times faster than it clusters, on the benchmark
+// batch) while the one before it clusters.
 std::vector<int32_t> piece_cuts(const uint32_t* sizes, int32_t n_events, int64_t n) {
   const int64_t k = std::min<int64_t>({kMaxPieces, n / kPieceMinPoints, n_events});
+  std::vector<int64_t> ends;  // cumulative shares
+  int64_t shares = 0;
+  for (int64_t p = 0; p < k; ++p)
+    ends.push_back(shares += std::min<int64_t>(p + 1, 3));
   std::vector<int32_t> cuts{0};
   int64_t acc = 0;
   for (int32_t e = 0; e < n_events; ++e) {
     acc += sizes[e];
-    const int64_t p = (int64_t)cuts.size();  // the cut after this event would end piece p - 1
-    if (p < k && e + 1 < n_events && acc * k >= p * n)
+    const size_t p = cuts.size() - 1;  // the piece this event ends up in
+    if ((int64_t)p + 1 < k && e + 1 < n_events && acc * shares >= ends[p] * n)
       cuts.push_back(e + 1);
   }
   cuts.push_back(n_events);
