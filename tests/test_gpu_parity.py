@@ -374,18 +374,26 @@ def test_host_and_device_entry_points_agree():
     assert same_partition(a["ci"], b["ci"])
 
 
-def _pipelined_against_device(ev, sizes, prm, kernel):
+def _pipelined_against_device(ev, sizes, prm, kernel, unc=None, tags=None):
     import torch
     n = ev.n
     h = clue.PointsHost(ev.coords, ev.weights)
     h.is_seed = np.zeros(n, np.int32)
     h.rho = np.zeros(n, np.float32)
     h.nearest_higher = np.zeros(n, np.int32)
+    if unc is not None:
+        h.set_density_uncertainty(unc)
+    if tags is not None:
+        h.set_tags(tags)
     ch = clue.Clusterer(*prm)
     ch.make_clusters(h, clue.EuclideanMetric(), kernel, batch_item_sizes=sizes,
                      grid_mode=clue.GRID_PER_EVENT)
     dev = torch.device("cuda", 0)
+    on_dev = lambda a, t: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev, t)
     d = clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev),
+                          density_uncertainty=on_dev(unc, torch.float32),
+                          tags=None if tags is None else on_dev(np.asarray(tags, np.int64).astype(np.int32),
+                                                                torch.int32),
                           outputs=("cluster_index", "is_seed", "rho", "nearest_higher"))
     cd = clue.Clusterer(*prm)
     cd.make_clusters(d, clue.EuclideanMetric(), kernel, batch_item_sizes=sizes,
@@ -422,6 +430,16 @@ def test_pipelined_host_batch_equals_the_device_batch_3d_gaussian():
     if ev.n < 1 << 23:
         pytest.skip("the 3-D batch came out below the pipelining size")
     assert _pipelined_against_device(ev, sizes, (3.0, 10.0, 4.0), clue.GaussianKernel(1.0, 1.0)) >= 2
+
+
+def test_pipelined_host_batch_with_uncertainty_and_tags():
+    # the tagged nearest-higher path and per-point uncertainties, staged piece by piece
+    ev, sizes = W.batch_2d(640, 4096, 32768, seed=63)
+    rng = np.random.default_rng(64)
+    unc = rng.uniform(0.5, 1.5, ev.n).astype(np.float32)
+    tags = rng.permutation(ev.n).astype(np.uint32)
+    assert _pipelined_against_device(ev, sizes, (1.5, 5.0, 1.5), clue.FlatKernel(0.5), unc=unc,
+                                     tags=tags) >= 2
 
 
 def test_small_host_batch_runs_in_one_piece():
