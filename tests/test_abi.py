@@ -126,3 +126,11 @@ def test_tuning_defaults_and_struct_layout():
     assert (t.density_union_x16_2d, t.density_union_x16_3d, t.label_jump_rounds) == (20, 1 << 20, -1)
     assert C.sizeof(L.Tuning) == 12
     assert L.load().clue_tuning_defaults(None) == L.ERR_INVALID_ARGUMENT
+
+
+def test_host_pieces_query_checks_its_arguments():
+    # a null workspace or output is rejected before any CUDA call
+    lib = L.load()
+    n = C.c_int32(-1)
+    assert lib.clue_workspace_host_pieces(None, C.byref(n)) == L.ERR_INVALID_ARGUMENT
+    assert n.value == -1
