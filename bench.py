@@ -135,7 +135,8 @@ def max_over_ranks(x: float, world: int) -> float:
 
 
 def cpu_reference(ev, sizes, budget_points: int, threads: int):
-    """Times the CPU restatement on the first events of the batch (bounded sample)."""
+    """Times the CPU restatement on the first events of the batch (bounded sample).
+    Returns (points/s, sample description, points, events, checker result)."""
     from oracle import oracle as O
     total, k = 0, 0
     while k < len(sizes) and total + int(sizes[k]) <= budget_points:
@@ -144,10 +145,30 @@ def cpu_reference(ev, sizes, budget_points: int, threads: int):
     k = max(k, 1)
     total = int(sizes[:k].sum())
     t0 = time.perf_counter()
-    O.make_clusters_batched(ev.coords[:, :total], ev.weights[:total], sizes[:k], 1.5, 5.0, 1.5,
-                            shared_grid=False, n_threads=threads)
+    res = O.make_clusters_batched(ev.coords[:, :total], ev.weights[:total], sizes[:k], 1.5, 5.0, 1.5,
+                                  shared_grid=False, n_threads=threads)
     dt = time.perf_counter() - t0
-    return total / dt, f"first {k} events of the batch ({total} points), all events clustered", total
+    return (total / dt, f"first {k} events of the batch ({total} points), all events clustered", total, k,
+            res)
+
+
+def parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, ref, n_points, n_events):
+    """Clusters the benchmark batch once more with every output requested and
+    compares the first `n_events` events (densities as bits, nearest higher,
+    seed flags, cluster ids) with the checker's result `ref` on those events;
+    the run's cluster ids must also equal those of the timed runs."""
+    import cluestering_b200 as clue
+    full = clue.PointsDevice(coords_d, weights_d)
+    algo.make_clusters(full, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=stream)
+    rho = full.rho[:n_points].cpu().numpy()
+    ci_all = full.cluster_index.cpu().numpy()
+    same = (np.array_equal(rho.view(np.int32), ref.rho.view(np.int32))
+            and np.array_equal(full.nearest_higher[:n_points].cpu().numpy(), ref.nearest_higher)
+            and np.array_equal(full.is_seed[:n_points].cpu().numpy(), ref.is_seed)
+            and np.array_equal(ci_all[:n_points], ref.cluster_index))
+    return {"events": int(n_events), "points": int(n_points), "identical": bool(same),
+            "timed_run_labels_identical": bool(np.array_equal(ci_all, timed_labels)),
+            "compared": "rho bits, nearest_higher, is_seed, cluster_index against the CPU checker"}
 
 
 def run_reference(args, world, rank):
@@ -161,7 +182,7 @@ def run_reference(args, world, rank):
         cpu_reference(ev, sizes, budget // 4, threads)
     vals = []
     for _ in range(args.steps):
-        v, sample, pts = cpu_reference(ev, sizes, budget, threads)
+        v, sample, pts, _, _ = cpu_reference(ev, sizes, budget, threads)
         vals.append(v)
     value = float(np.median(vals))
     line = {
@@ -256,8 +277,20 @@ def run_ours(args, world, rank, local):
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     e2e_ms = max_over_ranks(e2e_ms, world)
     e2e_value = R.job_throughput(points_all, e2e_ms)
-    same = bool(np.array_equal(h.cluster_index, pts.cluster_index.cpu().numpy()))
+    timed_labels = pts.cluster_index.cpu().numpy()
+    same = bool(np.array_equal(h.cluster_index, timed_labels))
     pieces = algo_h.host_pieces()  # uploads and downloads overlap the clustering of other pieces
+
+    # ---- CPU checker on the batch's first events: baseline timing and parity sample -------------
+    parity = None
+    if rank == 0:
+        threads = os.cpu_count() or 1
+        cpu_val, cpu_sample, cpu_pts, cpu_k, cpu_res = cpu_reference(ev, sizes, args.cpu_sample_points,
+                                                                     threads)
+        parity = parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, cpu_res, cpu_pts,
+                               cpu_k)
+        del cpu_res
+        ser_val, ser_sample, _, _, _ = cpu_reference(ev, sizes, args.cpu_serial_points, 1)
 
     extras = {}
     if rank == 0 and not args.skip_extras:
@@ -268,7 +301,6 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return 0
-    cpu_val, cpu_sample, _ = cpu_reference(ev, sizes, args.cpu_sample_points, os.cpu_count() or 1)
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -293,8 +325,11 @@ def run_ours(args, world, rank, local):
                              "algorithmic bytes, traffic is ncu DRAM bytes per point scaled to "
                              "this launch"},
         "clocks": clocks.summary(),
-        "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": os.cpu_count() or 1,
-                         "kind": "port", "sample": cpu_sample},
+        "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": threads,
+                         "kind": "port", "sample": cpu_sample,
+                         "serial_1_core": {"value": ser_val, "unit": "points/s", "cores": 1,
+                                           "sample": ser_sample}},
+        "parity_sample": parity,
     }
     line.update(extras)
     print(json.dumps(line), flush=True)
@@ -505,6 +540,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-points", type=int, default=3_000_000)
+    ap.add_argument("--cpu-serial-points", type=int, default=600_000,
+                    help="sample of the one-core checker timing (the serial backend's setting)")
     ap.add_argument("--plain-events", type=int, default=4096)
     ap.add_argument("--events", type=int, default=4096,
                     help="events per batch (4096 is the benchmark; fewer only for profiling)")

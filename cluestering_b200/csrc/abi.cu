@@ -38,9 +38,6 @@ clue_status fail_cuda(cudaError_t e, const char* where) {
 // Tables
 // ---------------------------------------------------------------------------
 
-namespace {
-constexpr int kChunkPoints = 4096;
-
 // core/detail/SetupTiles.hpp:30-34.
 bool grid_shape(int D, int64_t n, int ppt, int32_t* k_out, int64_t* T_out) {
   const int64_t nt = (n + ppt - 1) / ppt;
@@ -71,7 +68,6 @@ void fill_grid(GridDesc* g, int D, int32_t k, int64_t T) {
     s *= k;
   }
 }
-}  // namespace
 
 bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode, int32_t ppt,
                   HostTables* t, RunShape* sh, const char** err) {

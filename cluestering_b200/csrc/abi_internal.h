@@ -56,6 +56,15 @@ struct clue_workspace {
 
 namespace clue_impl {
 
+// Points per block of the extents and binning kernels (one chunk each).
+constexpr int kChunkPoints = 4096;
+// Tile grid of an event of n points in D dimensions with ppt points per tile
+// (core/detail/SetupTiles.hpp:30-34): the smallest k with k^D tiles >= n / ppt.
+// False when the grid does not fit int32 tile ids.
+bool grid_shape(int D, int64_t n, int ppt, int32_t* k_out, int64_t* T_out);
+// A grid descriptor of k per dimension and T = k^D tiles, last dimension fastest.
+void fill_grid(GridDesc* g, int D, int32_t k, int64_t T);
+
 clue_status fail(clue_status s, const std::string& msg);
 clue_status fail_cuda(cudaError_t e, const char* where);
 clue_status check_params(const clue_params* p);

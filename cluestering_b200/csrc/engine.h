@@ -159,6 +159,10 @@ cudaError_t launch_clusters_csr(const DeviceBuffers& b, int64_t n, const int32_t
 
 int scan_blocks_for(int64_t n);
 
+// Streaming multiprocessors of the current device, queried once per device;
+// grids of the grid-stride kernels are capped at a multiple of it.
+int sm_count();
+
 // Kernel launches enqueued by the calling thread since its last reset: every
 // launch site counts itself, and a run resets the count before it starts.
 void reset_launch_count();

@@ -11,6 +11,7 @@
 //   NH sweep      : nearest higher, the reference's comparisons and tie-breaks
 //   seeds/labels  : exclusive scan of the seed flags (seed k = k-th seed in
 //                   index order gets cluster id k), roots by pointer jumping.
+#include <atomic>
 #include <cfloat>
 #include <cuda/atomic>
 
@@ -762,7 +763,7 @@ __global__ void k_localize(const EventDesc* events, const int32_t* point_event,
 
 int grid_for(int64_t n, int per_block = kThreads) {
   const int64_t b = (n + per_block - 1) / per_block;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)sm_count() * 16));
 }
 
 cudaError_t fill32(void* p, int64_t words, uint32_t v, cudaStream_t st) {
@@ -798,14 +799,14 @@ cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* i
   const int64_t warps_per_block = kThreads / 32;
   const int blocks =
       (int)std::max<int64_t>(1, std::min<int64_t>((n_segments + warps_per_block - 1) / warps_per_block,
-                                                  148 * 16));
+                                                  (int64_t)sm_count() * 16));
   k_tile_sort<<<blocks, kThreads, 0, st>>>(offsets, n_segments, ids, b.large_tiles, large_count,
                                            event_exact, b.point_event, b.events);
-  k_tile_sort_large<<<148 * 8, kThreads, 0, st>>>(offsets, b.large_tiles, large_count, ids,
+  k_tile_sort_large<<<sm_count() * 8, kThreads, 0, st>>>(offsets, b.large_tiles, large_count, ids,
                                                   b.oversize, oversize_count, event_exact,
                                                   b.point_event, b.events);
-  k_tile_merge<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, ids, b.merge_tmp);
-  k_tile_merge_copy<<<148, kThreads, 0, st>>>(offsets, b.oversize, oversize_count, b.merge_tmp,
+  k_tile_merge<<<sm_count(), kThreads, 0, st>>>(offsets, b.oversize, oversize_count, ids, b.merge_tmp);
+  k_tile_merge_copy<<<sm_count(), kThreads, 0, st>>>(offsets, b.oversize, oversize_count, b.merge_tmp,
                                               ids);
   count_launches(4);
   return cudaGetLastError();
@@ -814,6 +815,21 @@ cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* i
 thread_local int64_t t_launches = 0;
 
 }  // namespace
+
+int sm_count() {
+  constexpr int kDevices = 64;
+  static std::atomic<int> cache[kDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices)
+    return 148;  // no usable device: the launch that follows reports the error
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      return 148;
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
 
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
 

@@ -1,8 +1,6 @@
 // noalloc.cu — clue_make_clusters_device_noalloc: the single-event run with
 // every scratch buffer carved from one file-scope device array instead of a
 // workspace allocation. The launch sequence is the library's usual one.
-#include <cstring>
-#include <mutex>
 
 #include "abi_internal.h"
 
@@ -15,29 +13,18 @@ namespace {
 // sequence clears everything that has to start at zero.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CLUE_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-char* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of this device's copy of g_noalloc_scratch. In host code the
-// array's name is only a host-side stand-in, so the address has to be looked up
-// once per device, with that device current.
+// Device address of the current device's copy of g_noalloc_scratch. In host
+// code the array's name is only a host-side stand-in, so the address is looked
+// up with the device current. The lookup allocates nothing and runs on every
+// call, so the address stays right after cudaDeviceReset or a new primary
+// context loads the module elsewhere; the first call on a device may load the
+// library's device code.
 clue_status scratch_for_current_device(char** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess)
-    return fail_cuda(e, "cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices)
-    return fail(CLUE_ERR_OUT_OF_RANGE, "device index out of range for the no-allocation path");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return fail_cuda(e, "cudaGetSymbolAddress");
-    g_scratch_addr[dev] = static_cast<char*>(p);
-  }
-  *out = g_scratch_addr[dev];
+    return fail_cuda(e, "cudaGetSymbolAddress of the no-allocation scratch");
+  *out = static_cast<char*>(p);
   return CLUE_OK;
 }
 
@@ -71,24 +58,15 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
                     std::to_string(pts->n) + ")");
   const int D = pts->ndim;
   const int64_t n = pts->n;
-  // Tile grid of the event (core/detail/SetupTiles.hpp:30-34).
+  // Tile grid of the event (core/detail/SetupTiles.hpp:30-34), by the same
+  // helpers the workspace path builds its tables with.
   const int ppt = params->points_per_tile > 0 ? params->points_per_tile : 128;
-  const int64_t nt = (n + ppt - 1) / ppt;
-  int64_t k = 1, T = 1;
-  for (;; ++k) {
-    T = 1;
-    for (int d = 0; d < D; ++d)
-      T *= k;
-    if (T >= nt)
-      break;
-  }
+  int32_t k = 0;
+  int64_t T = 0;
+  if (!grid_shape(D, n, ppt, &k, &T))
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "tile grid too large");
   GridDesc g;
-  std::memset(&g, 0, sizeof g);
-  g.k = (int32_t)k;
-  g.T = (int32_t)T;
-  for (int d = D - 1, stride = 1; d >= 0; --d, stride *= (int)k)
-    g.stride[d] = stride;
-  constexpr int kChunkPoints = 4096;
+  fill_grid(&g, D, k, T);
   RunShape sh;
   sh.D = D;
   sh.n = n;
@@ -122,7 +100,12 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   carve_buffers(&b, cap, base);
 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  cudaError_t e = cudaMemsetAsync(b.status, 0, sizeof(uint32_t), st);
+  // a failure of an earlier call whose status was not read would otherwise
+  // show up as this call's error
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail_cuda(e, "a CUDA error left pending before this run");
+  e = cudaMemsetAsync(b.status, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess)
     return fail_cuda(e, "status reset");
   k_noalloc_tables<<<(sh.n_chunks + 31) / 32, 32, 0, st>>>(g, (int32_t)n, kChunkPoints, b.grids,

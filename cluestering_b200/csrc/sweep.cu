@@ -31,7 +31,7 @@ constexpr float kSqrt2 = 1.41421356237309504880f;
 
 int grid_for(int64_t n) {
   const int64_t b = (n + kThreads - 1) / kThreads;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)sm_count() * 16));
 }
 
 // Search box of point s: bins [inf, sup] per dimension (TilesView.hpp:77-87),
@@ -1699,16 +1699,16 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
   // With cells, k_cells writes the density work order; k_work_order is still
   // needed for the nearest-higher order when the cell search is off (tags).
   if (!a.nh_cells) {
-    const int blocks = (int)std::min<int64_t>(a.n_tiles, 148 * 16);
+    const int blocks = (int)std::min<int64_t>(a.n_tiles, (int64_t)sm_count() * 16);
     CLUE_DISPATCH_D(D, k_work_order, blocks, kThreads, 0, st)
     count_launches(1);
   }
   if (a.nh_pos) {
     const int warp_blocks =
-        (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, 148 * 32));
+        (int)std::max<int64_t>(1, std::min<int64_t>((a.n_tiles + kCellWarps - 1) / kCellWarps, (int64_t)sm_count() * 32));
     // blocks for the large tiles: at most one per tile that can be large
     const int large_blocks =
-        (int)std::max<int64_t>(1, std::min<int64_t>(a.n / (kLargeTilePoints + 1), 148 * 24));
+        (int)std::max<int64_t>(1, std::min<int64_t>(a.n / (kLargeTilePoints + 1), (int64_t)sm_count() * 24));
     if (D == 2)
       k_cells<2><<<large_blocks + warp_blocks, kCellWarps * 32, 0, st>>>(p, a, large_blocks);
     else

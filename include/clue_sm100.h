@@ -250,8 +250,10 @@ clue_status clue_make_clusters_batched_host(clue_workspace* ws, const clue_param
  * in device memory on every GPU that loads it, for the life of the process.
  *   - At most CLUE_NOALLOC_MAX_POINTS points per call; larger events are
  *     rejected with CLUE_ERR_INVALID_ARGUMENT before any GPU work.
- *   - The first call on a device looks up that device's copy of the array;
- *     make it before capturing any stream.
+ *   - Every call looks up the current device's copy of the array (a lookup
+ *     that allocates nothing), so the address stays valid after
+ *     cudaDeviceReset. The first call on a device may load the library's
+ *     device code; make it before capturing any stream.
  *   - All calls share the array: calls whose GPU work overlaps (different
  *     streams, or different host threads, on one device) race and corrupt each
  *     other. Serialise them, e.g. on one stream.

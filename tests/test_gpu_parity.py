@@ -133,6 +133,26 @@ def test_large_2d_event_full_size():
     check(ev.coords, ev.weights, 1.5, 8.0, 2.0, path="device")
 
 
+def test_full_benchmark_batch_against_checker():
+    # The benchmark's own batch: 4,096 events of log-uniform size in
+    # [256, 65,536] (46.5 M points), one grid per event, through the device and
+    # the host entry points (the latter pipelined in pieces), against the
+    # checker on all host cores.
+    import os
+    ev, sizes = W.batch_2d()
+    o = run_oracle(ev.coords, ev.weights, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT,
+                   threads=os.cpu_count() or 1)
+    for path in ("device", "host"):
+        g = run_gpu(ev.coords, ev.weights, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT,
+                    path=path)
+        assert_identical(g, o)
+        offsets, n_keys = g["clusterer"].getSampleAssociations()
+        assert n_keys == len(sizes)
+        assert np.array_equal(offsets, expected_sample_offsets(o, len(sizes)))
+        assert np.array_equal(g["clusterer"].getSeeds(), o.seeds)
+        del g
+
+
 def test_batch_of_mixed_size_events_per_event_grid():
     ev, sizes = W.batch_2d(64, 256, 8192, seed=21)
     w = np.random.default_rng(3).exponential(1.0, ev.n).astype(np.float32)
@@ -254,9 +274,27 @@ def test_batched_fixed_batch_size_counts():
     assert g["ci"].max() + 1 == 10 * truth_count("data_1024")
     offsets, n_keys = g["clusterer"].getSampleAssociations()
     assert n_keys == 10
-    assert offsets[-1] == g["ci"].max() + 1
+    assert np.array_equal(offsets, expected_sample_offsets(o, 10))
     seeds = g["clusterer"].getSeeds()
     assert np.array_equal(seeds, o.seeds)
+
+
+def expected_sample_offsets(o, n_events):
+    """The checker's seed -> event associations (core/detail/Clusterer.hpp:221-242)
+    as the event -> cluster-id CSR offsets that getSampleAssociations returns:
+    cluster k is seed k, so the clusters of event e are a contiguous id range."""
+    ea = np.asarray(o.event_associations)
+    assert np.all(np.diff(ea) >= 0)
+    return np.concatenate([[0], np.cumsum(np.bincount(ea, minlength=n_events))]).astype(np.int32)
+
+
+def test_sample_associations_full_csr_mixed_batch():
+    ev, sizes = W.batch_2d(48, 256, 8192, seed=5)
+    for mode in (clue.GRID_PER_EVENT, clue.GRID_SHARED):
+        g, o = check(ev.coords, ev.weights, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=mode)
+        offsets, n_keys = g["clusterer"].getSampleAssociations()
+        assert n_keys == len(sizes)
+        assert np.array_equal(offsets, expected_sample_offsets(o, len(sizes)))
 
 
 @pytest.mark.parametrize("name", ["data_4096", "data_32768"])

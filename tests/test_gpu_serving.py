@@ -5,6 +5,7 @@ are submitted while earlier batches run; each result must equal, bit for bit,
 the single-event call on that event alone.
 """
 
+import os
 import threading
 import time
 
@@ -81,20 +82,36 @@ def test_results_are_the_same_alone_and_in_the_mix(pinned, timed):
         assert np.array_equal(p.cluster_index, a.cluster_index)
 
 
-def test_served_results_match_the_checker():
-    evs = _events(6, seed=3)
-    with clue.Server([P2, P3]) as srv:
-        pts = [_host_points(ev) for _, ev in evs]
-        for (prof, _), p in zip(evs, pts):
+def _checker(prof, ev, **extra):
+    kw = dict(kernel="flat", kernel_params=(0.5,)) if prof == 0 else \
+        dict(kernel="gaussian", kernel_params=(1.0, 1.0))
+    prm = (1.5, 5.0, 1.5) if prof == 0 else (3.0, 10.0, 4.0)
+    return O.make_clusters(ev.coords, ev.weights, *prm, exp_mode=O.EXP_CLUE,
+                           n_threads=os.cpu_count() or 1, **kw, **extra)
+
+
+def _assert_checker(p, o):
+    assert np.array_equal(p.rho.view(np.int32), o.rho.view(np.int32))
+    assert np.array_equal(p.nearest_higher, o.nearest_higher)
+    assert np.array_equal(p.is_seed, o.is_seed)
+    assert np.array_equal(p.cluster_index, o.cluster_index)
+
+
+def test_served_mix_matches_the_checker():
+    # 200 events of the serving mix itself (80 % 2-D flat, 20 % 3-D Gaussian,
+    # sizes log-uniform in [1,024, 262,144]), submitted at once so that they
+    # share batches, each compared with the checker on that event alone.
+    evs = list(W.serving_mix(200, seed=17))
+    prof_of = [0 if ev.ndim == 2 else 1 for ev in evs]
+    pts = [_host_points(ev, pinned=True) for ev in evs]
+    with clue.Server([P2, P3], budget_bytes=8 << 30, max_inflight=4, max_batch_events=64,
+                     max_batch_points=2_000_000) as srv:
+        for prof, p in zip(prof_of, pts):
             srv.submit(prof, p)
         srv.drain()
-    for (prof, ev), p in zip(evs, pts):
-        kw = dict(kernel="flat", kernel_params=(0.5,)) if prof == 0 else \
-            dict(kernel="gaussian", kernel_params=(1.0, 1.0))
-        prm = (1.5, 5.0, 1.5) if prof == 0 else (3.0, 10.0, 4.0)
-        o = O.make_clusters(ev.coords, ev.weights, *prm, exp_mode=O.EXP_CLUE, **kw)
-        assert np.array_equal(p.cluster_index, o.cluster_index)
-        assert np.array_equal(p.nearest_higher, o.nearest_higher)
+        assert srv.stats()["batches"] < len(evs)
+    for prof, ev, p in zip(prof_of, evs, pts):
+        _assert_checker(p, _checker(prof, ev))
 
 
 def test_arrivals_while_batches_run():

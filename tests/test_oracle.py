@@ -5,6 +5,7 @@ the fixtures extracted into tests/golden/.
 """
 
 import math
+import os
 import struct
 
 import numpy as np
@@ -137,16 +138,33 @@ def test_clue_expf_special_values():
     assert abs(O.expf(-100.0) - _f32(math.exp(-100.0))) <= 2 ** -149
 
 
-def test_exp_choice_moves_densities_within_tolerance():
-    # The GPU path uses clue_expf; the reference's serial backend uses libm's
-    # expf. Densities agree within the 1e-5 relative tolerance.
+def _exp_cases():
     from cluestering_b200 import workloads as W
-    ev = W.layered_3d(3000, seed=5)
-    a = O.make_clusters(ev.coords, ev.weights, 3.0, 10.0, 4.0, kernel="gaussian",
-                        kernel_params=(1.0, 1.0), exp_mode=O.EXP_CLUE)
-    b = O.make_clusters(ev.coords, ev.weights, 3.0, 10.0, 4.0, kernel="gaussian",
-                        kernel_params=(1.0, 1.0), exp_mode=O.EXP_LIBM)
+    gauss = dict(dc=3.0, rhoc=10.0, dm=4.0, kernel="gaussian", kernel_params=(1.0, 1.0))
+    yield "layered_3d_10000", W.layered_3d(), gauss
+    yield "layered_3d_262144", W.layered_3d(262144, seed=11), gauss
+    yield "blobs_2d_exponential_kernel", \
+        W.blobs(1 << 15, 40, 0.0, 100.0, 1.0, 0.1, seed=4, weights="exponential"), \
+        dict(dc=1.5, rhoc=5.0, dm=1.5, kernel="exponential", kernel_params=(1.0, 1.0))
+
+
+@pytest.mark.parametrize("case", ["layered_3d_10000", "layered_3d_262144", "blobs_2d_exponential_kernel"])
+def test_exp_choice_keeps_nearest_higher_and_partitions(case):
+    # The GPU path and this checker evaluate the Gaussian and exponential
+    # kernels with clue_expf; the reference's serial backend calls libm's
+    # std::exp (internal/math/exp/exp.hpp:19-29). The two differ in the last
+    # bit of some exponentials, so densities may differ within the 1e-5
+    # relative tolerance, while nearest-higher indices, seed flags and the
+    # partition must come out identical.
+    ev, prm = next((e, p) for name, e, p in _exp_cases() if name == case)
+    threads = min(8, os.cpu_count() or 1)
+    a = O.make_clusters(ev.coords, ev.weights, exp_mode=O.EXP_CLUE, n_threads=threads, **prm)
+    b = O.make_clusters(ev.coords, ev.weights, exp_mode=O.EXP_LIBM, n_threads=threads, **prm)
     np.testing.assert_allclose(a.rho, b.rho, rtol=1e-5)
+    assert np.array_equal(a.nearest_higher, b.nearest_higher)
+    assert np.array_equal(a.is_seed, b.is_seed)
+    assert same_partition(a.cluster_index, b.cluster_index)
+    assert a.n_clusters > 0
 
 
 def test_shared_and_per_event_grids_agree_on_exact_sums():

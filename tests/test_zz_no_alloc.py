@@ -35,7 +35,8 @@ def _outputs(p):
 def _noalloc(algo, p, stream, status):
     prm = algo.params()
     pts = clue.api._points_struct(p)
-    return L.load().clue_make_clusters_device_noalloc(C.byref(prm), C.byref(pts), status.data_ptr(),
+    return L.load().clue_make_clusters_device_noalloc(C.byref(prm), C.byref(pts),
+                                                      None if status is None else status.data_ptr(),
                                                       stream.cuda_stream)
 
 
@@ -104,3 +105,47 @@ def test_noalloc_rejects_events_above_the_limit():
     rc = _noalloc(algo, p, torch.cuda.current_stream(), status)
     assert rc == L.ERR_INVALID_ARGUMENT
     assert b"at most 16384 points" in L.load().clue_last_error()
+
+
+def test_noalloc_leaves_free_device_memory_unchanged():
+    # The defining property: once the library's device code is loaded (the
+    # first call), further calls take no device memory at all.
+    torch = pytest.importorskip("torch")
+    ev = W.single_2d(12000, seed=75)
+    algo = clue.Clusterer(1.5, 5.0, 1.5)
+    pts = [_device_points(ev, torch) for _ in range(4)]
+    stream = torch.cuda.Stream()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert _noalloc(algo, pts[0], stream, status) == L.OK, L.load().clue_last_error()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for p in pts:
+        assert _noalloc(algo, p, stream, status) == L.OK, L.load().clue_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    ref = _outputs(pts[0])
+    for p in pts[1:]:
+        for a, b in zip(_outputs(p), ref):
+            assert np.array_equal(a, b)
+
+
+def test_noalloc_without_status_and_in_one_dimension():
+    # device_status may be NULL; a 1-D event takes the path without the cell
+    # layout. Both match the workspace path.
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(76)
+    x = np.concatenate([rng.normal(c, 0.5, 900) for c in (5.0, 20.0, 40.0)] +
+                       [rng.uniform(0.0, 50.0, 300)]).astype(np.float32)[None, :]
+    w = rng.exponential(1.0, x.shape[1]).astype(np.float32)
+    for coords, weights, prm in [(x, w, (1.0, 4.0, 1.5)),
+                                 (W.single_2d(8000, seed=77).coords, np.ones(8000, np.float32), (1.5, 5.0, 1.5))]:
+        ev = W.Event(coords, weights)
+        algo = clue.Clusterer(*prm)
+        ref = _device_points(ev, torch)
+        algo.make_clusters(ref)
+        got = _device_points(ev, torch)
+        stream = torch.cuda.Stream()
+        assert _noalloc(algo, got, stream, None) == L.OK, L.load().clue_last_error()
+        stream.synchronize()
+        for a, b in zip(_outputs(got), _outputs(ref)):
+            assert np.array_equal(a, b)
