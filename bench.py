@@ -403,9 +403,11 @@ def run_extras(args, ev, sizes, local, stream, hbm_peak):
 
 def run_serving(args, local):
     """Serving form on a mixed stream: saturated throughput, then Poisson
-    arrivals at fractions of it, with per-event latency (completion - arrival).
-    The plain per-event form (one synchronous call per event) runs on the same
-    stream for comparison."""
+    arrivals at fractions of it, with per-event latency (completion - arrival),
+    and the configured stream of `serve_stream_total` arrivals at half of the
+    peak load. Arrivals cycle through a pool of `serve_events` distinct
+    generated events. The plain per-event form (one synchronous call per event)
+    runs on the same pool for comparison."""
     import torch
 
     import cluestering_b200 as clue
@@ -423,15 +425,17 @@ def run_serving(args, local):
               clue.GaussianKernel(1.0, 1.0))]
     prof_of = [0 if ev.ndim == 2 else 1 for ev in evs]
     total = sum(ev.n for ev in evs)
+    mean_pts = total / len(evs)
     cfg = dict(device=local, budget_bytes=40 << 30, max_inflight=args.serve_inflight,
                max_batch_events=args.serve_batch_events, max_batch_points=args.serve_batch_points,
                linger_us=args.serve_linger_us, max_batch_ms=args.serve_batch_ms,
                priority_ms=args.serve_priority_ms)
     out = {"events": len(evs), "points": total, "mix": "80% 2-D single_2d-style, 20% 3-D layered_3d-style",
-           "sizes": "log-uniform [1024, 262144]", "config": cfg, "stream": args.serve_stream,
+           "sizes": "log-uniform [1024, 262144]", "config": cfg,
            "method": "each server first clusters 64 events (not counted), which also seeds its cost "
-                     "model; peak = all events submitted at once; loads = a Poisson stream of "
-                     "`stream` arrivals cycling through the events"}
+                     "model; peak = all pool events submitted at once; loads = Poisson arrivals "
+                     "cycling through the pool of distinct events; the configured stream is "
+                     "`stream_total` arrivals at half of the peak load"}
     warm = min(64, len(evs))
 
     def warm_up(srv):
@@ -446,15 +450,19 @@ def run_serving(args, local):
             srv.submit(prof_of[i], p)
         srv.drain()
         peak = total / (time.perf_counter() - t0)
+        st = srv.stats()
     out["peak_points_per_s"] = peak
-    peak_events = peak / (total / len(evs))
-    # arrival k is event k mod len(evs); repeats of one event are len(evs) arrivals
-    # apart, long after the earlier one completed at these loads
-    order = [k % len(evs) for k in range(args.serve_stream)]
-    stream_points = sum(evs[i].n for i in order)
-    loads = []
+    out["budget"] = {"budget_bytes": cfg["budget_bytes"], "slot_bytes": st["slot_bytes"],
+                     "resident_pool_bytes": st["resident_pool_bytes"],
+                     "max_batch_points": st["max_batch_points"]}
+    peak_events = peak / mean_pts
     rng = np.random.default_rng(0)
-    for f in args.serve_loads:
+
+    def offered(f, arrivals):
+        # arrival k is pool event k mod len(evs); repeats of one event are
+        # len(evs) arrivals apart, long after the earlier one completed
+        order = [k % len(evs) for k in range(arrivals)]
+        points = sum(evs[i].n for i in order)
         with clue.Server(profs, **cfg) as srv:
             warm_up(srv)
             gaps = rng.exponential(1.0 / (f * peak_events), size=len(order))
@@ -469,12 +477,19 @@ def run_serving(args, local):
             dt = time.perf_counter() - t0
             lat = srv.latencies_ms()[warm:]
             st = srv.stats()
-        loads.append({"load": f, "points_per_s": stream_points / dt, "p50_ms": float(np.percentile(lat, 50)),
-                      "p99_ms": float(np.percentile(lat, 99)), "batches": st["batches"]})
-    out["loads"] = loads
-    half = min(loads, key=lambda r: abs(r["load"] - 0.5))
+        return {"load": f, "arrivals": arrivals, "points_per_s": points / dt,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "batches": st["batches"], "resident_bytes_peak": st["resident_bytes_peak"],
+                "admission_waits": st["admission_waits"]}
+
+    out["loads"] = [offered(f, args.serve_stream) for f in args.serve_loads]
+    if args.serve_stream_total > 0:
+        out["configured_stream"] = offered(0.5, args.serve_stream_total)
+        half = out["configured_stream"]
+    else:
+        half = min(out["loads"], key=lambda r: abs(r["load"] - 0.5))
     out["p50_ms_at_half_load"], out["p99_ms_at_half_load"] = half["p50_ms"], half["p99_ms"]
-    # plain per-event on the same stream
+    # plain per-event on the same pool
     algos = [profs[0][1], profs[1][1]]
     for i in range(min(16, len(evs))):
         algos[prof_of[i]].make_clusters(pts[i], profs[prof_of[i]][2], profs[prof_of[i]][3])
@@ -545,14 +560,17 @@ def main():
     ap.add_argument("--plain-events", type=int, default=4096)
     ap.add_argument("--events", type=int, default=4096,
                     help="events per batch (4096 is the benchmark; fewer only for profiling)")
-    ap.add_argument("--serve-events", type=int, default=1500)
+    ap.add_argument("--serve-events", type=int, default=3000,
+                    help="distinct generated events the serving arrivals cycle through")
     ap.add_argument("--serve-inflight", type=int, default=4)
     ap.add_argument("--serve-batch-events", type=int, default=64)
     ap.add_argument("--serve-batch-points", type=int, default=2_000_000)
     ap.add_argument("--serve-linger-us", type=int, default=200)
     ap.add_argument("--serve-batch-ms", type=float, default=2.0)
     ap.add_argument("--serve-priority-ms", type=float, default=1.5)
-    ap.add_argument("--serve-stream", type=int, default=4000)
+    ap.add_argument("--serve-stream", type=int, default=12000, help="arrivals per offered load")
+    ap.add_argument("--serve-stream-total", type=int, default=200_000,
+                    help="arrivals of the configured stream at half of the peak load (0: skip)")
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--skip-extras", action="store_true")
     ap.add_argument("--case", choices=["one-tile", "layered-3d"], default=None,

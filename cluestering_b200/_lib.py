@@ -62,7 +62,8 @@ class Points(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("density_union_x16_2d", C.c_int32), ("density_union_x16_3d", C.c_int32),
-                ("label_jump_rounds", C.c_int32)]
+                ("label_jump_rounds", C.c_int32), ("cell_points", C.c_int32),
+                ("density_shape", C.c_int32), ("nh_shape", C.c_int32)]
 
 
 class ServerProfile(C.Structure):
@@ -92,6 +93,11 @@ class ServerStats(C.Structure):
         ("latency_p50_ms", C.c_double),
         ("latency_p99_ms", C.c_double),
         ("latency_max_ms", C.c_double),
+        ("resident_bytes_peak", C.c_int64),
+        ("resident_pool_bytes", C.c_int64),
+        ("slot_bytes", C.c_int64),
+        ("admission_waits", C.c_int64),
+        ("max_batch_points", C.c_int64),
     ]
 
 

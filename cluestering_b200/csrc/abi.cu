@@ -38,6 +38,14 @@ clue_status fail_cuda(cudaError_t e, const char* where) {
 // Tables
 // ---------------------------------------------------------------------------
 
+int32_t sort_runs(int64_t n, int64_t T, int32_t* len) {
+  const int64_t by_size = (n + 1023) / 1024;
+  const int64_t by_matrix = T > 0 ? n / T : n;
+  const int64_t runs = std::max<int64_t>(1, std::min(by_size, by_matrix));
+  *len = (int32_t)std::max<int64_t>(1, (n + runs - 1) / runs);
+  return (int32_t)runs;
+}
+
 // core/detail/SetupTiles.hpp:30-34.
 bool grid_shape(int D, int64_t n, int ppt, int32_t* k_out, int64_t* T_out) {
   const int64_t nt = (n + ppt - 1) / ppt;
@@ -95,7 +103,7 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
     t->grids.resize(1);
     fill_grid(&t->grids[0], D, k, T);
     for (int e = 0; e < B; ++e) {
-      t->events[e] = EventDesc{(int32_t)begin, (int32_t)sizes[e], (int32_t)(T * e), 0};
+      t->events[e] = EventDesc{(int32_t)begin, (int32_t)sizes[e], (int32_t)(T * e), 0, 0, 0, 0, 0};
       begin += sizes[e];
     }
     tiles = T * B;
@@ -109,7 +117,7 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
         return false;
       }
       fill_grid(&t->grids[e], D, k, T);
-      t->events[e] = EventDesc{(int32_t)begin, (int32_t)sizes[e], (int32_t)tiles, e};
+      t->events[e] = EventDesc{(int32_t)begin, (int32_t)sizes[e], (int32_t)tiles, e, 0, 0, 0, 0};
       begin += sizes[e];
       tiles += T;
       if (tiles >= INT32_MAX) {
@@ -123,6 +131,23 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
     for (int32_t c = ev.begin; c < ev.begin + ev.n; c += kChunkPoints)
       t->chunks.push_back(Chunk{e, c, std::min(ev.begin + ev.n, c + kChunkPoints)});
   }
+  // Stable binning layout: runs of each event, their warps and count matrices.
+  int64_t warps = 0, entries = 0;
+  int32_t max_tiles = 0;
+  for (int e = 0; e < B; ++e) {
+    EventDesc& ev = t->events[e];
+    const int64_t T = t->grids[ev.grid].T;
+    ev.sort_chunks = sort_runs(ev.n, T, &ev.sort_len);
+    ev.sort_first = (int32_t)std::min<int64_t>(warps, INT32_MAX);
+    ev.sort_base = (int32_t)std::min<int64_t>(entries, INT32_MAX);
+    warps += ev.sort_chunks;
+    entries += T * ev.sort_chunks;
+    max_tiles = (int32_t)std::max<int64_t>(max_tiles, std::min<int64_t>(T, INT32_MAX));
+  }
+  sh->stable = max_tiles <= kStableMaxTiles && entries <= N && warps < INT32_MAX;
+  sh->sort_warps = (int32_t)std::min<int64_t>(warps, INT32_MAX);
+  sh->sort_entries = entries;
+  sh->max_event_tiles = max_tiles;
   sh->D = D;
   sh->n = N;
   sh->n_tiles = tiles;
@@ -378,6 +403,9 @@ clue_tuning default_tuning() {
   t.density_union_x16_2d = 20;
   t.density_union_x16_3d = 1 << 20;
   t.label_jump_rounds = -1;
+  t.cell_points = 2;
+  t.density_shape = 0;
+  t.nh_shape = 0;
   return t;
 }
 
@@ -385,6 +413,9 @@ RunParams make_run_params(const clue_params* p, const clue_points* pts, const cl
   RunParams r{};
   r.union_x16 = pts->ndim == 3 ? t.density_union_x16_3d : t.density_union_x16_2d;
   r.jump_rounds = t.label_jump_rounds;
+  r.cell_points = t.cell_points;
+  r.dens_shape = t.density_shape;
+  r.nh_shape = t.nh_shape;
   r.D = pts->ndim;
   r.dc = p->dc;
   r.rhoc = p->rhoc;
@@ -1070,6 +1101,11 @@ clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tun
     return fail(CLUE_ERR_INVALID_ARGUMENT, "union thresholds must be >= 0");
   if (tuning->label_jump_rounds < -1 || tuning->label_jump_rounds > 4)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "label_jump_rounds must be in [-1, 4]");
+  if (tuning->cell_points < 1 || tuning->cell_points > 8)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "cell_points must be in [1, 8]");
+  if (tuning->density_shape < 0 || tuning->density_shape > 2 || tuning->nh_shape < 0 ||
+      tuning->nh_shape > 2)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "density_shape and nh_shape must be in [0, 2]");
   ws->tuning = *tuning;
   return CLUE_OK;
 }
@@ -1266,11 +1302,17 @@ clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* param
       }
     }
   };
-  // The union threshold matters on the packed 2-D/3-D path only.
+  // The union threshold, the cell size and the sweeps' block shapes matter on
+  // the packed 2-D/3-D path only.
   if (points->ndim == 2)
     try_field(&clue_tuning::density_union_x16_2d, {0, 12, 16, 20, 24, 32, 48, 1 << 20});
   else if (points->ndim == 3)
     try_field(&clue_tuning::density_union_x16_3d, {0, 16, 24, 32, 48, 64, 1 << 20});
+  if (points->ndim == 2 || points->ndim == 3) {
+    try_field(&clue_tuning::cell_points, {1, 2, 3, 4});
+    try_field(&clue_tuning::density_shape, {0, 1, 2});
+    try_field(&clue_tuning::nh_shape, {0, 1, 2});
+  }
   try_field(&clue_tuning::label_jump_rounds, {0, 1, 2, 3, 4});
   for (auto& x : ev)
     cudaEventDestroy(x);

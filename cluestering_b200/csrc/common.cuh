@@ -43,7 +43,18 @@ struct EventDesc {
   int32_t n;          // number of points
   int32_t tile_base;  // first global tile id of this event
   int32_t grid;       // index into the grid table
+  // Stable tile binning: the event's points form sort_chunks runs of sort_len
+  // consecutive points, run c binned by warp sort_first + c; its count matrix
+  // (tiles x runs, tile-major) starts at entry sort_base.
+  int32_t sort_first;
+  int32_t sort_chunks;
+  int32_t sort_len;
+  int32_t sort_base;
 };
+
+// Tiles of one event the stable binning handles: each warp keeps a counter per
+// tile of its event in shared memory (48 KB per block at most).
+constexpr int kStableMaxTiles = 12288;
 
 // A run of consecutive points of one event, processed by one block.
 struct Chunk {
@@ -89,6 +100,12 @@ struct RunParams {
   int32_t union_x16;
   // Pointer-jumping rounds before the label walk; -1: by size.
   int32_t jump_rounds;
+  // Average points per cell of the sweeps' cell layout (1..8).
+  int32_t cell_points;
+  // Block shapes of the density sweep and of the nearest-higher cell search
+  // (clue_tuning::density_shape, nh_shape).
+  int32_t dens_shape;
+  int32_t nh_shape;
 };
 
 // ---------------------------------------------------------------------------

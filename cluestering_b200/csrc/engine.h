@@ -95,7 +95,19 @@ struct RunShape {
   int32_t n_events = 0;
   int32_t n_grids = 0;
   int32_t n_chunks = 0;
+  // Stable tile binning (one warp per run of consecutive points of an event):
+  // usable when every event has at most kStableMaxTiles tiles and the count
+  // matrices of all events hold at most n entries.
+  bool stable = false;
+  int32_t sort_warps = 0;
+  int64_t sort_entries = 0;
+  int32_t max_event_tiles = 0;
 };
+
+// Runs of the stable binning for an event of n points in T tiles: as many as
+// keep the event's count matrix (T x runs) within n entries, at most one per
+// 1,024 points, at least one. Returns the run count; *len = points per run.
+int32_t sort_runs(int64_t n, int64_t T, int32_t* len);
 
 // Pointers of one run's inputs and outputs (device memory).
 struct RunIO {

@@ -181,6 +181,161 @@ __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, cons
 }
 
 // ---------------------------------------------------------------------------
+// Stable tile binning: one warp per run of consecutive points of one event,
+// runs of an event in index order. Binning counts each run's points per tile
+// into the event's count matrix (tiles x runs, tile-major); an exclusive scan
+// of all matrices turns every entry into the sorted position of that run's
+// first point in that tile; the scatter then places each run's points in
+// index order from those positions. Every tile thus lists its points in
+// ascending index, the order the reference's serial fill produces
+// (data_structures/detail/AssociationMap.hpp:63-81), with no sort.
+// ---------------------------------------------------------------------------
+
+// Event of stable-binning warp w: the last event whose first warp is <= w.
+__device__ __forceinline__ int sort_event_of(const EventDesc* events, int n_events, int w) {
+  int lo = 0, hi = n_events - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (events[mid].sort_first <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Tile ids and per-run tile counts; also the exact-sum bounds of the event
+// (flat kernel, when event_exact is given), as in k_bin. s_col holds one
+// counter per tile of the warp's event (max_tiles per warp).
+__global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs x, const EventDesc* events,
+                                                         int n_events, int n_warps, const GridDesc* grids,
+                                                         int32_t* tile_of, int32_t* point_event,
+                                                         int32_t* matrix, int max_tiles,
+                                                         const float* weight, int32_t* event_exact) {
+  extern __shared__ int s_col[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= n_warps)
+    return;  // whole warps only: nothing below synchronises the block
+  int* col = s_col + (threadIdx.x >> 5) * max_tiles;
+  const int e = sort_event_of(events, n_events, w);
+  const EventDesc ev = events[e];
+  const GridDesc& g = grids[ev.grid];
+  const int c = w - ev.sort_first;
+  const int T = g.T;
+  for (int t = lane; t < T; t += 32)
+    col[t] = 0;
+  __syncwarp();
+  const int begin = ev.begin + c * ev.sort_len;
+  const int end = min(ev.begin + ev.n, begin + ev.sort_len);
+  const bool bounds = event_exact && p.kernel_kind == CLUE_KERNEL_FLAT;
+  int lsb = INT_MAX, bad = 0;
+  uint32_t vb = 0, wb = 0;
+  for (int base = begin; base < end; base += 32) {
+    const int i = base + lane;
+    const bool valid = i < end;
+    int t = -1;
+    if (valid) {
+      int b = 0;
+      for (int d = 0; d < p.D; ++d)
+        b += g.stride[d] * get_bin(g, p, x.p[d][i], d);
+      t = b;
+      tile_of[i] = ev.tile_base + t;
+      point_event[i] = e;
+      if (bounds) {
+        const float wt = weight[i];
+        const float v = __fmul_rn(p.kernel_p0, wt);  // a neighbour's fl(flat * w_j)
+        const int bd = !(wt >= 0.0f) || signbit(wt) || isinf(wt) || isinf(v);
+        bad |= bd;
+        if (!bd) {
+          if (v > 0.0f)
+            lsb = min(lsb, lsb_exponent(v));
+          if (wt > 0.0f)
+            lsb = min(lsb, lsb_exponent(wt));
+          vb = max(vb, __float_as_uint(v));
+          wb = max(wb, __float_as_uint(wt));
+        }
+      }
+    }
+    const unsigned mask = __match_any_sync(kFull, t);
+    if (valid && lane == __ffs(mask) - 1)
+      col[t] += __popc(mask);
+    __syncwarp();  // the next round's leaders read these counters
+  }
+  for (int t = lane; t < T; t += 32)
+    matrix[(int64_t)ev.sort_base + (int64_t)t * ev.sort_chunks + c] = col[t];
+  if (bounds) {
+    lsb = __reduce_min_sync(kFull, lsb);
+    vb = __reduce_max_sync(kFull, vb);
+    wb = __reduce_max_sync(kFull, wb);
+    bad = __any_sync(kFull, bad);
+    if (lane == 0) {
+      int32_t* st = event_exact + 4 * e;
+      atomicMin(&st[0], lsb);
+      atomicMax(reinterpret_cast<unsigned*>(&st[1]), vb);
+      atomicMax(reinterpret_cast<unsigned*>(&st[2]), wb);
+      if (bad)
+        atomicOr(&st[3], 1);
+    }
+  }
+}
+
+// Places each run's points from its scanned matrix column. The first run of
+// each event also writes the event's tile offsets and lists its tiles of more
+// than kLargeTilePoints points (for k_cells).
+__global__ void __launch_bounds__(kThreads) k_scatter_stable(const EventDesc* events, int n_events,
+                                                             int n_warps, const GridDesc* grids,
+                                                             const int32_t* tile_of, const int32_t* matrix,
+                                                             int max_tiles, int32_t* perm,
+                                                             int32_t* tile_offset, int64_t n_tiles,
+                                                             int32_t n_points, int32_t* large,
+                                                             int32_t* large_count) {
+  extern __shared__ int s_col[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= n_warps)
+    return;
+  int* col = s_col + (threadIdx.x >> 5) * max_tiles;
+  const int e = sort_event_of(events, n_events, w);
+  const EventDesc ev = events[e];
+  const int c = w - ev.sort_first;
+  const int T = grids[ev.grid].T;
+  for (int t = lane; t < T; t += 32)
+    col[t] = matrix[(int64_t)ev.sort_base + (int64_t)t * ev.sort_chunks + c];
+  __syncwarp();
+  if (c == 0) {
+    for (int t = lane; t < T; t += 32) {
+      const int start = col[t];
+      tile_offset[ev.tile_base + t] = start;
+      const int next = t + 1 < T ? col[t + 1] : ev.begin + ev.n;
+      if (next - start > kLargeTilePoints)
+        large[atomicAdd(large_count, 1)] = ev.tile_base + t;
+    }
+    if (w == 0 && lane == 0)
+      tile_offset[n_tiles] = n_points;
+    __syncwarp();
+  }
+  const int begin = ev.begin + c * ev.sort_len;
+  const int end = min(ev.begin + ev.n, begin + ev.sort_len);
+  for (int base = begin; base < end; base += 32) {
+    const int i = base + lane;
+    const bool valid = i < end;
+    const int t = valid ? tile_of[i] - ev.tile_base : -1;
+    const unsigned mask = __match_any_sync(kFull, t);
+    const int leader = __ffs(mask) - 1;
+    int pos = 0;
+    if (valid && lane == leader) {
+      pos = col[t];
+      col[t] = pos + __popc(mask);
+    }
+    pos = __shfl_sync(kFull, pos, leader);
+    if (valid)
+      perm[pos + __popc(mask & lanemask_lt())] = i;
+    __syncwarp();  // the next round's leaders read these cursors
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Single-pass exclusive scan with decoupled look-back.
 // Each block takes a ticket (so every predecessor is already running), scans
 // kScanTile elements, publishes its aggregate, then walks back over its
@@ -927,20 +1082,40 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // counting sort by tile
   CLUE_MARK(1);
-  CLUE_CHECK(fill32(b.tile_count, sh.n_tiles, 0, st));
-  k_bin<<<sh.n_chunks, kThreads, 0, st>>>(prm, x, b.chunks, b.events, b.grids, b.tile_of,
-                                           b.point_event, b.tile_count, io.weight, exact);
-  CLUE_LAUNCHED();
-  CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));
-  k_copy32<<<grid_for(sh.n_tiles), kThreads, 0, st>>>((uint32_t*)b.tile_cursor,
-                                                     (const uint32_t*)b.tile_offset, sh.n_tiles);
-  CLUE_LAUNCHED();
-  k_scatter<<<grid_for(n), kThreads, 0, st>>>(b.tile_of, n, b.tile_cursor, b.perm);
-  CLUE_LAUNCHED();
-  // Exact-sum events need no ascending order within their tiles when nothing
-  // else on this run reads it (flat kernel, cell path: no user tags).
-  const bool order_free_tiles = sweep_cells_path(prm) && prm.kernel_kind == CLUE_KERNEL_FLAT;
-  CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st, order_free_tiles ? exact : nullptr));
+  if (sh.stable) {
+    // Stable binning: runs of consecutive points, one warp each; the count
+    // matrices live in merge_tmp (at most n entries).
+    int32_t* matrix = b.merge_tmp;
+    const int wpb = std::max(1, std::min(kThreads / 32, (48 << 10) / (4 * std::max(1, sh.max_event_tiles))));
+    const int blocks = (sh.sort_warps + wpb - 1) / wpb;
+    const size_t smem = (size_t)wpb * sh.max_event_tiles * sizeof(int);
+    CLUE_CHECK(fill32(b.counters + 3, 1, 0, st));  // large-tile count
+    k_bin_stable<<<blocks, wpb * 32, smem, st>>>(prm, x, b.events, sh.n_events, sh.sort_warps, b.grids,
+                                                 b.tile_of, b.point_event, matrix,
+                                                 sh.max_event_tiles, io.weight, exact);
+    CLUE_LAUNCHED();
+    CLUE_CHECK(scan(matrix, matrix, sh.sort_entries, b.counters + 7, b, st));
+    k_scatter_stable<<<blocks, wpb * 32, smem, st>>>(b.events, sh.n_events, sh.sort_warps, b.grids,
+                                                     b.tile_of, matrix, sh.max_event_tiles, b.perm,
+                                                     b.tile_offset, sh.n_tiles, (int32_t)n,
+                                                     b.large_tiles, b.counters + 3);
+    CLUE_LAUNCHED();
+  } else {
+    CLUE_CHECK(fill32(b.tile_count, sh.n_tiles, 0, st));
+    k_bin<<<sh.n_chunks, kThreads, 0, st>>>(prm, x, b.chunks, b.events, b.grids, b.tile_of,
+                                             b.point_event, b.tile_count, io.weight, exact);
+    CLUE_LAUNCHED();
+    CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));
+    k_copy32<<<grid_for(sh.n_tiles), kThreads, 0, st>>>((uint32_t*)b.tile_cursor,
+                                                       (const uint32_t*)b.tile_offset, sh.n_tiles);
+    CLUE_LAUNCHED();
+    k_scatter<<<grid_for(n), kThreads, 0, st>>>(b.tile_of, n, b.tile_cursor, b.perm);
+    CLUE_LAUNCHED();
+    // Exact-sum events need no ascending order within their tiles when nothing
+    // else on this run reads it (flat kernel, cell path: no user tags).
+    const bool order_free_tiles = sweep_cells_path(prm) && prm.kernel_kind == CLUE_KERNEL_FLAT;
+    CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st, order_free_tiles ? exact : nullptr));
+  }
   CLUE_MARK(2);
   k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
                                              io.unc, io.tags, b.point_event, b.sorted_coords,

@@ -30,12 +30,13 @@ clue_status scratch_for_current_device(char** out) {
 
 // Writes the one-event tables into the scratch: grid, event and the chunks of
 // kChunkPoints points (the same split the allocating path builds on the host).
-__global__ void k_noalloc_tables(GridDesc g, int32_t n, int32_t chunk_points, GridDesc* grids,
+__global__ void k_noalloc_tables(GridDesc g, EventDesc ev, int32_t chunk_points, GridDesc* grids,
                                  EventDesc* events, Chunk* chunks, int32_t n_chunks) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t n = ev.n;
   if (i == 0) {
     grids[0] = g;
-    events[0] = EventDesc{0, n, 0, 0};
+    events[0] = ev;
   }
   if (i < n_chunks)
     chunks[i] = Chunk{0, i * chunk_points, min(n, (i + 1) * chunk_points)};
@@ -74,6 +75,13 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   sh.n_events = 1;
   sh.n_grids = 1;
   sh.n_chunks = (int32_t)((n + kChunkPoints - 1) / kChunkPoints);
+  // the one event and its stable-binning layout (as build_tables lays it out)
+  EventDesc ev{0, (int32_t)n, 0, 0, 0, 0, 0, 0};
+  ev.sort_chunks = sort_runs(n, T, &ev.sort_len);
+  sh.sort_warps = ev.sort_chunks;
+  sh.sort_entries = T * (int64_t)ev.sort_chunks;
+  sh.max_event_tiles = (int32_t)T;
+  sh.stable = T <= kStableMaxTiles && sh.sort_entries <= n;
 
   bool any_sigma = false;
   for (int d = 0; d < D; ++d)
@@ -108,8 +116,8 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   e = cudaMemsetAsync(b.status, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess)
     return fail_cuda(e, "status reset");
-  k_noalloc_tables<<<(sh.n_chunks + 31) / 32, 32, 0, st>>>(g, (int32_t)n, kChunkPoints, b.grids,
-                                                           b.events, b.chunks, sh.n_chunks);
+  k_noalloc_tables<<<(sh.n_chunks + 31) / 32, 32, 0, st>>>(g, ev, kChunkPoints, b.grids, b.events,
+                                                           b.chunks, sh.n_chunks);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return fail_cuda(e, "table setup");
 

@@ -428,7 +428,9 @@ __device__ __forceinline__ void for_each_candidate(const SweepArgs& a, const Gri
 // a warp can reach; the nearest-higher search visits them nearest-first.
 // ---------------------------------------------------------------------------
 
-constexpr int kCellTarget = 2;     // average points per cell
+// Average points per cell: a launch tuning (clue_tuning::cell_points, 1..8,
+// default 2). Cells only order and prune the candidates of the sweeps, so the
+// choice never changes a result.
 constexpr int kCellSlots = 2048;   // cells per tile at most (45^2, 12^3)
 constexpr int kCellWarps = 8;      // warps per block of k_cells
 
@@ -438,12 +440,12 @@ __host__ __device__ constexpr int cell_dim_max() {
 }
 
 template <int D>
-__device__ __forceinline__ int cells_per_dim(int m) {
+__device__ __forceinline__ int cells_per_dim(int m, int target) {
   int s = 1;
   while (s < cell_dim_max<D>()) {
     const int u = s + 1;
     const int vol = D == 2 ? u * u : u * u * u;
-    if (vol * kCellTarget > m)
+    if (vol * target > m)
       break;
     s = u;
   }
@@ -898,13 +900,13 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
 // lane reads each record from shared memory. The stream is the box's rows in
 // order, each a contiguous range of sorted positions, i.e. the reference's
 // summation order. Other warps read candidates from global memory.
-template <int D, int KIND>
-__global__ void __launch_bounds__(kThreads, 4) k_density_fast(const RunParams p, const SweepArgs a) {
-  __shared__ __align__(16) float4 s_ring[kThreads / 32][kRing][kChunk];
-  __shared__ int s_off[kThreads / 32][kMaxStream + 1];
-  __shared__ int s_qa[kThreads / 32][kMaxStream];
-  __shared__ int s_seg[kThreads / 32][kMaxSegs];
-  __shared__ int4 s_tinfo[kThreads / 32][kMaxUnionTiles];
+template <int D, int KIND, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_density_fast(const RunParams p, const SweepArgs a) {
+  __shared__ __align__(16) float4 s_ring[NT / 32][kRing][kChunk];
+  __shared__ int s_off[NT / 32][kMaxStream + 1];
+  __shared__ int s_qa[NT / 32][kMaxStream];
+  __shared__ int s_seg[NT / 32][kMaxSegs];
+  __shared__ int4 s_tinfo[NT / 32][kMaxUnionTiles];
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_dens;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1332,7 +1334,7 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
     return;
   const EventDesc ev = a.events[a.sevt[begin]];
   const GridDesc& g = a.grids[ev.grid];
-  const int s = cells_per_dim<D>(m);
+  const int s = cells_per_dim<D>(m, p.cell_points);
   float lo[D], inv[D];
   int own[D];
   {
@@ -1483,7 +1485,7 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
 // a dense tile of thousands of points does not hold up the launch on one warp;
 // they come first so that the heaviest tiles do not run as a tail. The other
 // blocks give one warp to each smaller tile.
-constexpr int kWarpCellSlots = kLargeTilePoints / kCellTarget;  // s^D * 2 <= m <= 256
+constexpr int kWarpCellSlots = kLargeTilePoints;  // s^D <= m <= 256 (at least 1 point per cell)
 template <int D>
 __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a,
                                                           int large_blocks) {
@@ -1546,9 +1548,8 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
 // 256 threads per SM measured 8.3 ms on the 46.5 M-point batch against 9.4 ms
 // at 5 and 10.8 ms at 4, small spills included. The 3-D form, with more state
 // per lane, stays at 4.
-template <int D>
-__global__ void __launch_bounds__(kThreads, D == 2 ? 8 : 4) k_nearest_higher_cells(const RunParams p,
-                                                                   const SweepArgs a) {
+template <int D, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunParams p, const SweepArgs a) {
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_nh;
   const int lane = threadIdx.x & 31;
@@ -1718,22 +1719,64 @@ cudaError_t launch_work_order(int D, const RunParams& p, const SweepArgs& a, cud
   return cudaGetLastError();
 }
 
+// Grid of a persistent sweep: enough blocks of nt threads to cover n points,
+// at most `per_sm` per SM (the kernels take work items from a queue).
+int sweep_grid(int64_t n, int nt, int per_sm) {
+  const int64_t b = (n + nt - 1) / nt;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)sm_count() * per_sm));
+}
+
+// Block shapes of the density sweep (clue_tuning::density_shape):
+// 0: 256 threads, 4 blocks per SM; 1: 128 threads, 8 per SM; 2: 256 threads, 3 per SM.
+template <int D, int KIND>
+void launch_density_kind(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
+  switch (p.dens_shape) {
+    case 1:
+      k_density_fast<D, KIND, 128, 8><<<sweep_grid(a.n, 128, 32), 128, 0, st>>>(p, a);
+      break;
+    case 2:
+      k_density_fast<D, KIND, 256, 3><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
+      break;
+    default:
+      k_density_fast<D, KIND, 256, 4><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
+      break;
+  }
+}
+
 template <int D>
 cudaError_t launch_density_fast(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   k_pack_density<D><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
   count_launches(2);  // this and the density kernel below
   switch (p.kernel_kind) {
     case CLUE_KERNEL_FLAT:
-      k_density_fast<D, CLUE_KERNEL_FLAT><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      launch_density_kind<D, CLUE_KERNEL_FLAT>(p, a, st);
       break;
     case CLUE_KERNEL_GAUSSIAN:
-      k_density_fast<D, CLUE_KERNEL_GAUSSIAN><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      launch_density_kind<D, CLUE_KERNEL_GAUSSIAN>(p, a, st);
       break;
     default:
-      k_density_fast<D, CLUE_KERNEL_EXPONENTIAL><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      launch_density_kind<D, CLUE_KERNEL_EXPONENTIAL>(p, a, st);
       break;
   }
   return cudaGetLastError();
+}
+
+// Block shapes of the nearest-higher cell search (clue_tuning::nh_shape):
+// 0: 256 threads with 8 blocks per SM in 2-D, 4 in 3-D; 1: 256 threads, 6 per
+// SM; 2: 128 threads with 16 blocks per SM in 2-D, 8 in 3-D.
+template <int D>
+void launch_nh_cells(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
+  switch (p.nh_shape) {
+    case 1:
+      k_nearest_higher_cells<D, 256, 6><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
+      break;
+    case 2:
+      k_nearest_higher_cells<D, 128, D == 2 ? 16 : 8><<<sweep_grid(a.n, 128, 32), 128, 0, st>>>(p, a);
+      break;
+    default:
+      k_nearest_higher_cells<D, 256, D == 2 ? 8 : 4><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
+      break;
+  }
 }
 
 cudaError_t launch_density(int D, const RunParams& p, const SweepArgs& a, cudaStream_t st) {
@@ -1752,9 +1795,9 @@ cudaError_t launch_nearest_higher(int D, const RunParams& p, const SweepArgs& a,
   count_launches(1);  // one kernel on every path below
   if (a.nh_cells) {
     if (D == 2)
-      k_nearest_higher_cells<2><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      launch_nh_cells<2>(p, a, st);
     else
-      k_nearest_higher_cells<3><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
+      launch_nh_cells<3>(p, a, st);
     return cudaGetLastError();
   }
   if (sweep_fast_path(p)) {

@@ -193,6 +193,18 @@ typedef struct {
    * each point walks to its seed (0..4); -1 picks by size (none below 2^18
    * points, 2 below 2^22, else 3). */
   int32_t label_jump_rounds;
+  /* Sweeps of 2-D and 3-D Euclidean runs: average points per cell of the cell
+   * layout that orders and prunes the candidates inside each tile (1..8;
+   * default 2). The tile grid itself stays the reference's (128 points per
+   * tile): it decides the search boxes and the order of the density sums. */
+  int32_t cell_points;
+  /* Block shape of the density sweep: 0 = 256 threads with 4 blocks per SM,
+   * 1 = 128 threads with 8, 2 = 256 threads with 3. */
+  int32_t density_shape;
+  /* Block shape of the nearest-higher cell search: 0 = 256 threads with 8
+   * blocks per SM in 2-D (4 in 3-D), 1 = 256 threads with 6, 2 = 128 threads
+   * with 16 in 2-D (8 in 3-D). */
+  int32_t nh_shape;
 } clue_tuning;
 
 /* Defaults: the values the library ships with. */
@@ -200,7 +212,7 @@ clue_status clue_tuning_defaults(clue_tuning* out);
 /* The workspace's current choices (defaults until set or autotuned). */
 clue_status clue_workspace_get_tuning(const clue_workspace* ws, clue_tuning* out);
 /* CLUE_ERR_INVALID_ARGUMENT if a field is out of range (a negative threshold,
- * jump rounds outside -1..4). */
+ * jump rounds outside -1..4, cell_points outside 1..8, a shape outside 0..2). */
 clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tuning);
 /* Autotuner: runs make_clusters on these device points (the single-event form
  * when event_sizes is NULL, else the batched form with grid_mode) under
@@ -334,12 +346,15 @@ clue_status clue_memcpy_async(void* dst, const void* src, size_t bytes, int32_t 
 /* A request loop with continuous batching (no counterpart in the reference,
  * whose callers run one make_clusters per event and thread, as in
  * benchmark/throughput/worker.cpp:17-39). Events are submitted from host memory
- * as they arrive. A scheduler thread groups pending events of one profile by
- * size, admits a batch when a stream slot is free and the batch's device
- * footprint fits the memory budget, and runs it while earlier batches are
- * still on the GPU; each event completes on its own. Every event gets the
- * single-event result (CLUE_GRID_PER_EVENT semantics), so a result does not
- * depend on what it was batched with. */
+ * as they arrive. A scheduler thread admits them in arrival order by device
+ * memory: an event is admitted when its input planes fit the resident pool
+ * (the budget left after the stream slots), and its points are uploaded at
+ * once and stay on the device until the event completes. Admitted events of
+ * one profile and one set of per-point options are grouped by size into
+ * batches; a batch starts when a stream slot is free and runs while earlier
+ * batches are still on the GPU; each event completes on its own. Every event
+ * gets the single-event result (CLUE_GRID_PER_EVENT semantics), so a result
+ * does not depend on what it was batched with. */
 typedef struct clue_server clue_server;
 
 /* Events of one profile share ndim and clustering parameters. */
@@ -350,8 +365,11 @@ typedef struct {
 
 typedef struct {
   int32_t device;
-  size_t budget_bytes;      /* device memory the server may hold (all slots) */
-  int32_t max_inflight;     /* batches on the GPU at once (one stream each) */
+  /* Device memory the server may hold: the stream slots (each a workspace and
+   * the planes of one batch, together at most half of it) and the resident
+   * pool of admitted events (the rest). */
+  size_t budget_bytes;
+  int32_t max_inflight;     /* batches on the GPU at once (one stream slot each) */
   int32_t max_batch_events; /* events per batch */
   int64_t max_batch_points; /* points per batch (0: derived from the budget) */
   int32_t linger_us;        /* how long a small batch may wait for company */
@@ -370,17 +388,24 @@ typedef struct {
 typedef struct {
   int64_t submitted, completed, batches;
   int64_t points_completed;
-  int64_t inflight_bytes_peak;
+  int64_t inflight_bytes_peak;  /* peak device bytes of busy slots plus resident events */
   double latency_p50_ms, latency_p99_ms, latency_max_ms;
+  int64_t resident_bytes_peak;  /* peak bytes of the resident pool in use */
+  int64_t resident_pool_bytes;  /* size of the resident pool */
+  int64_t slot_bytes;           /* device bytes of all stream slots */
+  int64_t admission_waits;      /* times the oldest waiting event did not fit yet */
+  int64_t max_batch_points;     /* points one batch can hold */
 } clue_server_stats;
 
 clue_status clue_server_create(clue_server** server, const clue_server_config* config,
                                const clue_server_profile* profiles, int32_t n_profiles);
-/* Queues one event of the given profile. The host buffers must stay valid (and
- * unmodified) until the event completes; pinned buffers are copied by DMA,
- * pageable ones through the server's pinned staging. Outputs land in
- * points->cluster_index (and the optional outputs). An event larger than a
- * batch can hold is rejected with CLUE_ERR_OUT_OF_MEMORY. */
+/* Queues one event of the given profile, with the per-point options the
+ * reference's points take (sigma per dimension, density uncertainty, tags:
+ * PointsHost.hpp:217-244). The host buffers must stay valid (and unmodified)
+ * until the event completes; pinned buffers are copied by DMA, pageable ones
+ * through the server's pinned staging. Outputs land in points->cluster_index
+ * (and the optional outputs). An event larger than a batch or the resident
+ * pool can hold is rejected with CLUE_ERR_OUT_OF_MEMORY. */
 clue_status clue_server_submit(clue_server* server, int32_t profile, const clue_points* points,
                                uint64_t* ticket);
 /* CLUE_OK when the event completed, CLUE_ERR_NOT_READY otherwise. */

@@ -488,9 +488,12 @@ def test_small_host_batch_runs_in_one_piece():
 # ---- launch tuning: results must not depend on it ---------------------------------------------
 
 TUNINGS = [
-    dict(density_union_x16_2d=0, density_union_x16_3d=0, label_jump_rounds=0),
-    dict(density_union_x16_2d=1 << 20, density_union_x16_3d=1 << 20, label_jump_rounds=4),
-    dict(density_union_x16_2d=16, density_union_x16_3d=24, label_jump_rounds=1),
+    dict(density_union_x16_2d=0, density_union_x16_3d=0, label_jump_rounds=0, cell_points=1,
+         density_shape=1, nh_shape=2),
+    dict(density_union_x16_2d=1 << 20, density_union_x16_3d=1 << 20, label_jump_rounds=4, cell_points=8,
+         density_shape=2, nh_shape=1),
+    dict(density_union_x16_2d=16, density_union_x16_3d=24, label_jump_rounds=1, cell_points=3,
+         density_shape=0, nh_shape=0),
 ]
 
 
@@ -502,6 +505,16 @@ def test_results_do_not_depend_on_tuning_2d(tuning):
     c.set_tuning(**tuning)
     assert c.get_tuning() == tuning
     check(ev.coords, w, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT, clusterer=c)
+
+
+@pytest.mark.parametrize("tuning", TUNINGS)
+def test_results_do_not_depend_on_tuning_exact_sums(tuning):
+    # unit weights: every event takes the exact-sum density over the cells
+    ev, sizes = W.batch_2d(48, 256, 32768, seed=33)
+    c = clue.Clusterer(1.5, 5.0, 1.5)
+    c.set_tuning(**tuning)
+    check(ev.coords, ev.weights, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=clue.GRID_PER_EVENT, clusterer=c,
+          path="device")
 
 
 @pytest.mark.parametrize("tuning", TUNINGS)
@@ -520,6 +533,12 @@ def test_set_tuning_rejects_out_of_range():
         c.set_tuning(density_union_x16_2d=-1)
     with pytest.raises(ValueError):
         c.set_tuning(label_jump_rounds=5)
+    with pytest.raises(ValueError):
+        c.set_tuning(cell_points=0)
+    with pytest.raises(ValueError):
+        c.set_tuning(density_shape=3)
+    with pytest.raises(ValueError):
+        c.set_tuning(nh_shape=-1)
     with pytest.raises(KeyError):
         c.set_tuning(points_per_tile=64)
 

@@ -147,10 +147,64 @@ def test_submit_rejects_what_the_server_cannot_take():
             srv.submit(0, clue.PointsHost(big.coords, big.weights))
         with pytest.raises(ValueError):
             srv.submit(0, clue.PointsHost(np.vstack([ev.coords, ev.coords[:1]]), ev.weights))
-        p = clue.PointsHost(ev.coords, ev.weights)
-        p.set_tags(np.arange(ev.n))
-        with pytest.raises(ValueError):
-            srv.submit(0, p)
+
+
+def _with_options(ev, kind, rng):
+    """Host points of `ev` carrying per-point options (PointsHost.hpp:217-244)."""
+    p = _host_points(ev, pinned=kind % 2 == 0)
+    if kind in (1, 3):
+        p.set_density_uncertainty(rng.uniform(0.5, 1.5, ev.n).astype(np.float32))
+    if kind in (2, 3):
+        p.set_tags(rng.permutation(ev.n).astype(np.int64))
+    if kind == 4:
+        p.set_sigma(0, rng.uniform(0.1, 0.6, ev.n).astype(np.float32))
+    return p
+
+
+def test_served_events_with_sigma_uncertainty_and_tags():
+    # Events carrying uncertainties, tags or sigma share batches only with
+    # events that carry the same options; each equals the checker's result
+    # on that event alone with the same options.
+    rng = np.random.default_rng(41)
+    evs = _events(40, seed=41)
+    kinds = [k % 5 for k in range(len(evs))]
+    pts = [_with_options(ev, kind, rng) for (_, ev), kind in zip(evs, kinds)]
+    with clue.Server([P2, P3], max_inflight=3, max_batch_events=8, budget_bytes=2 << 30,
+                     linger_us=300) as srv:
+        for (prof, _), p in zip(evs, pts):
+            srv.submit(prof, p)
+        srv.drain()
+    for (prof, ev), p, kind in zip(evs, pts, kinds):
+        extra = {}
+        if p.density_uncertainty is not None:
+            extra["unc"] = p.density_uncertainty
+        if p.tags is not None:
+            extra["tags"] = p.tags
+        if kind == 4:
+            extra["sigma"] = [p.sigma[0]] + [None] * (ev.ndim - 1)
+        _assert_checker(p, _checker(prof, ev, **extra))
+
+
+def test_admission_by_device_memory_budget():
+    # A budget whose resident pool holds only a few events at a time: events
+    # wait on the host until earlier ones complete, and every one completes
+    # with the single-event result.
+    evs = _events(50, seed=43)
+    pts = [_host_points(ev, pinned=True) for _, ev in evs]
+    with clue.Server([P2, P3], max_inflight=2, max_batch_events=4, max_batch_points=65536,
+                     budget_bytes=96 << 20) as srv:
+        for (prof, _), p in zip(evs, pts):
+            srv.submit(prof, p)
+        srv.drain()
+        st = srv.stats()
+    assert st["completed"] == len(evs)
+    assert st["admission_waits"] > 0
+    assert 0 < st["resident_bytes_peak"] <= st["resident_pool_bytes"]
+    assert st["slot_bytes"] + st["resident_pool_bytes"] <= 96 << 20
+    for (prof, ev), p in zip(evs, pts):
+        a = _alone(prof, ev)
+        assert np.array_equal(p.cluster_index, a.cluster_index)
+        assert np.array_equal(p.rho.view(np.int32), a.rho.view(np.int32))
 
 
 def test_server_rejects_negative_time_targets():
