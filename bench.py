@@ -53,6 +53,12 @@ BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4
 # profiles/nearest_higher_and_cells_batch_2d_1024ev.md: 703.2 MB for nearest
 # higher; 10,621,973 points); a launch's traffic grows with the points it processes.
 DRAM_BYTES_PER_POINT = {"density": 86.9, "nearest_higher": 66.2}
+# Warp instructions per point of each sweep (smsp__inst_executed.sum / points),
+# from the same captures: 2.76 G for density, 1.72 G for nearest higher over
+# 10,621,973 points. The sweeps are bound by instruction issue: the issue
+# roofline is SMs x 4 schedulers x one warp instruction per cycle at the SM
+# clock sampled during the timed steps.
+INST_PER_POINT = {"density": 259.8, "nearest_higher": 161.9}
 
 
 def measured_peaks():
@@ -160,15 +166,19 @@ def parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, ref, n
     import cluestering_b200 as clue
     full = clue.PointsDevice(coords_d, weights_d)
     algo.make_clusters(full, batch_item_sizes=sizes, grid_mode=clue.GRID_PER_EVENT, stream=stream)
-    rho = full.rho[:n_points].cpu().numpy()
+    rho_all = full.rho.cpu().numpy()
+    rho = rho_all[:n_points]
     ci_all = full.cluster_index.cpu().numpy()
+    # unit weights, flat kernel: rho_i = 1 + 0.5 (candidates in range - 1), exactly
+    in_range = float((2.0 * (rho_all.astype(np.float64) - 1.0) + 1.0).sum())
     same = (np.array_equal(rho.view(np.int32), ref.rho.view(np.int32))
             and np.array_equal(full.nearest_higher[:n_points].cpu().numpy(), ref.nearest_higher)
             and np.array_equal(full.is_seed[:n_points].cpu().numpy(), ref.is_seed)
             and np.array_equal(ci_all[:n_points], ref.cluster_index))
-    return {"events": int(n_events), "points": int(n_points), "identical": bool(same),
-            "timed_run_labels_identical": bool(np.array_equal(ci_all, timed_labels)),
-            "compared": "rho bits, nearest_higher, is_seed, cluster_index against the CPU checker"}
+    return ({"events": int(n_events), "points": int(n_points), "identical": bool(same),
+             "timed_run_labels_identical": bool(np.array_equal(ci_all, timed_labels)),
+             "compared": "rho bits, nearest_higher, is_seed, cluster_index against the CPU checker"},
+            in_range)
 
 
 def run_reference(args, world, rank):
@@ -250,14 +260,16 @@ def run_ours(args, world, rank, local):
     n_clusters = algo.n_clusters()
     launches_per_run = algo.kernel_launches()  # counted by the library at each launch site
 
-    # ---- stage times of one profiled run (outside the timed region) -----------------------------
+    # ---- stage times and sweep statistics of one profiled run (outside the timed region) ---------
     algo.set_profiling(True)
     step()
     stage = algo.stage_ms()
+    sweeps = algo.sweep_stats()
     algo.set_profiling(False)
     dom = max(("density", "nearest_higher"), key=lambda k: stage[k])
     D = 2
     achieved = BYTES_PER_POINT[dom](D) * n_total / (stage[dom] * 1e-3) / 1e9
+    n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
 
     # ---- end to end through the host entry point ------------------------------------------------
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
@@ -279,6 +291,7 @@ def run_ours(args, world, rank, local):
     e2e_value = R.job_throughput(points_all, e2e_ms)
     timed_labels = pts.cluster_index.cpu().numpy()
     same = bool(np.array_equal(h.cluster_index, timed_labels))
+    in_range = None
     pieces = algo_h.host_pieces()  # uploads and downloads overlap the clustering of other pieces
 
     # ---- CPU checker on the batch's first events: baseline timing and parity sample -------------
@@ -287,8 +300,8 @@ def run_ours(args, world, rank, local):
         threads = os.cpu_count() or 1
         cpu_val, cpu_sample, cpu_pts, cpu_k, cpu_res = cpu_reference(ev, sizes, args.cpu_sample_points,
                                                                      threads)
-        parity = parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, cpu_res, cpu_pts,
-                               cpu_k)
+        parity, in_range = parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, cpu_res,
+                                         cpu_pts, cpu_k)
         del cpu_res
         ser_val, ser_sample, _, _, _ = cpu_reference(ev, sizes, args.cpu_serial_points, 1)
 
@@ -301,6 +314,32 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return 0
+    clk = clocks.summary()
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "traffic": DRAM_BYTES_PER_POINT[dom] * n_total,
+            "peak_kind": peak_kind,
+            "note": "the sweeps are instruction-issue bound, not HBM bound: each point tests hundreds "
+                    "of candidate records read from shared memory; achieved counts algorithmic bytes, "
+                    "traffic is ncu DRAM bytes per point scaled to this launch; `issue` is the bound "
+                    "they hit"}
+    f_hz = (clk["sm_mhz"] or 1965.0) * 1e6
+    roof["issue"] = {
+        k: {"warp_inst_per_point": INST_PER_POINT[k],
+            "achieved_warp_inst_per_s": INST_PER_POINT[k] * n_total / (stage[k] * 1e-3),
+            "peak_warp_inst_per_s": n_sms * 4 * f_hz,
+            "frac": INST_PER_POINT[k] * n_total / (stage[k] * 1e-3) / (n_sms * 4 * f_hz)}
+        for k in ("density", "nearest_higher")}
+    roof["issue_frac"] = roof["issue"][dom]["frac"]
+    roof["pairs"] = {
+        "density_candidate_tests_per_point": sweeps["density_tests"] / n_total,
+        "density_candidate_tests_per_s": sweeps["density_tests"] / (stage["density"] * 1e-3),
+        "density_in_range_per_point": in_range / n_total if in_range else None,
+        "density_in_range_pairs_per_s": in_range / (stage["density"] * 1e-3) if in_range else None,
+        "nearest_higher_members_tested_per_point": sweeps["nh_members_tested"] / n_total,
+        "nearest_higher_cells_checked_per_point": sweeps["nh_cells_checked"] / n_total,
+        "nearest_higher_member_tests_per_s": sweeps["nh_members_tested"] / (stage["nearest_higher"] * 1e-3),
+    }
+    roof["pairs_per_s"] = roof["pairs"]["density_in_range_pairs_per_s"]
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -315,16 +354,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": launches_per_run * args.steps,
         "n_clusters": n_clusters,
         "stage_ms": {k: round(v, 4) for k, v in stage.items()},
-        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": DRAM_BYTES_PER_POINT[dom] * n_total,
-                     "peak_kind": peak_kind,
-                     "note": "the sweeps are instruction-issue bound, not HBM bound: each point "
-                             "tests hundreds of candidate records (density: ~820 per warp, read "
-                             "from shared memory, 85% issue active in ncu); achieved counts "
-                             "algorithmic bytes, traffic is ncu DRAM bytes per point scaled to "
-                             "this launch"},
-        "clocks": clocks.summary(),
+        "roofline": roof,
+        "clocks": clk,
         "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": threads,
                          "kind": "port", "sample": cpu_sample,
                          "serial_1_core": {"value": ser_val, "unit": "points/s", "cores": 1,
@@ -390,6 +421,7 @@ def run_extras(args, ev, sizes, local, stream, hbm_peak):
     algo1.set_profiling(True)
     algo1.make_clusters(bp, stream=stream)
     st = algo1.stage_ms()
+    sweeps1 = algo1.sweep_stats()
     nb = BYTES_PER_POINT["pipeline"](2) * big.n
     out["single_event_1M"] = {
         "ms": ms, "points_per_s": big.n / (ms * 1e-3),
@@ -397,6 +429,8 @@ def run_extras(args, ev, sizes, local, stream, hbm_peak):
         "stage_ms": {k: round(v, 4) for k, v in st.items()},
         "density_gbs": BYTES_PER_POINT["density"](2) * big.n / (st["density"] * 1e-3) / 1e9,
         "nearest_higher_gbs": BYTES_PER_POINT["nearest_higher"](2) * big.n / (st["nearest_higher"] * 1e-3) / 1e9,
+        "density_candidate_tests_per_point": sweeps1["density_tests"] / big.n,
+        "nearest_higher_members_tested_per_point": sweeps1["nh_members_tested"] / big.n,
     }
     return out
 
@@ -525,6 +559,38 @@ def run_layered_3d(args):
     return 0
 
 
+def run_large_2d(args):
+    """The 1,048,576-point 2-D event (exponential weights, dc = 1.5, rhoc = 8,
+    dm = 2): median of 10 device-timed runs after warm-up, then stage times and
+    sweep statistics of one profiled run. Profiles capture its launches."""
+    import torch
+
+    import cluestering_b200 as clue
+    from cluestering_b200 import workloads as W
+    big = W.large_2d()
+    dev = torch.device("cuda", 0)
+    bp = clue.PointsDevice(torch.from_numpy(big.coords).to(dev), torch.from_numpy(big.weights).to(dev),
+                           outputs=("cluster_index",))
+    algo = clue.Clusterer(1.5, 8.0, 2.0)
+    stream = torch.cuda.Stream(device=dev)
+    for _ in range(max(3, args.warmup)):
+        algo.make_clusters(bp, stream=stream)
+    times = []
+    for _ in range(10):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        algo.make_clusters(bp, stream=stream, synchronize=False)
+        e.record(stream)
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e))
+    algo.set_profiling(True)
+    algo.make_clusters(bp, stream=stream)
+    print(json.dumps({"case": "large-2d", "points": big.n, "ms": float(np.median(times)),
+                      "stage_ms": {k: round(v, 4) for k, v in algo.stage_ms().items()},
+                      "sweeps": algo.sweep_stats(), "kernel_launches": algo.kernel_launches()}), flush=True)
+    return 0
+
+
 def run_one_tile(args):
     """One event of 16,384 points uniform in [0, 10]^2 with a single tile (dc = 0.3): every
     density warp streams the same 16,384 candidates, which isolates the per-candidate cost
@@ -573,16 +639,19 @@ def main():
                     help="arrivals of the configured stream at half of the peak load (0: skip)")
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.1, 0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--skip-extras", action="store_true")
-    ap.add_argument("--case", choices=["one-tile", "layered-3d"], default=None,
+    ap.add_argument("--case", choices=["one-tile", "layered-3d", "large-2d"], default=None,
                     help="profiling case instead of the benchmark: 'one-tile' clusters one "
                          "16,384-point event whose points all share one tile, so every warp of "
                          "the density sweep streams the same box; 'layered-3d' clusters one "
-                         "262,144-hit layered 3-D event (the serving mix's heaviest kind)")
+                         "262,144-hit layered 3-D event (the serving mix's heaviest kind); "
+                         "'large-2d' the 1,048,576-point event")
     args = ap.parse_args()
     if args.case == "one-tile":
         return run_one_tile(args)
     if args.case == "layered-3d":
         return run_layered_3d(args)
+    if args.case == "large-2d":
+        return run_large_2d(args)
     if args.impl == "reference":
         # CPU arm: rank 0 times the CPU restatement; other ranks have no work.
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")),

@@ -153,6 +153,7 @@ SIGNATURES = {
     "clue_server_drain": (C.c_int, [_P]),
     "clue_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
     "clue_server_latencies": (C.c_int, [_P, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    "clue_workspace_sweep_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.c_int32]),
     "clue_server_destroy": (C.c_int, [_P]),
 }
 

@@ -437,6 +437,16 @@ class Clusterer:
         L.check(L.load().clue_workspace_stage_ms(self._ws, ms, len(L.STAGES)))
         return dict(zip(L.STAGES, list(ms)))
 
+    def sweep_stats(self) -> dict:
+        """Candidate counts of the sweeps in the last run (needs set_profiling):
+        density candidate tests and work items, nearest-higher members tested,
+        cells checked and cells entered (clue_workspace_sweep_stats)."""
+        n = 5
+        v = (C.c_int64 * n)()
+        L.check(L.load().clue_workspace_sweep_stats(self._ws, v, n))
+        keys = ["density_tests", "density_items", "nh_members_tested", "nh_cells_checked", "nh_cells_entered"]
+        return dict(zip(keys, list(v)))
+
     def workspace_bytes(self) -> int:
         b = C.c_size_t()
         L.check(L.load().clue_workspace_bytes(self._workspace(), C.byref(b)))

@@ -38,12 +38,10 @@ clue_status fail_cuda(cudaError_t e, const char* where) {
 // Tables
 // ---------------------------------------------------------------------------
 
-int32_t sort_runs(int64_t n, int64_t T, int32_t* len) {
-  const int64_t by_size = (n + 1023) / 1024;
-  const int64_t by_matrix = T > 0 ? n / T : n;
-  const int64_t runs = std::max<int64_t>(1, std::min(by_size, by_matrix));
-  *len = (int32_t)std::max<int64_t>(1, (n + runs - 1) / runs);
-  return (int32_t)runs;
+int32_t sort_runs(int64_t n, int32_t* len) {
+  const int64_t runs = std::max<int64_t>(1, (n + kStableRun - 1) / kStableRun);
+  *len = kStableRun;
+  return (int32_t)std::min<int64_t>(runs, INT32_MAX);
 }
 
 // core/detail/SetupTiles.hpp:30-34.
@@ -137,14 +135,14 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
   for (int e = 0; e < B; ++e) {
     EventDesc& ev = t->events[e];
     const int64_t T = t->grids[ev.grid].T;
-    ev.sort_chunks = sort_runs(ev.n, T, &ev.sort_len);
+    ev.sort_chunks = sort_runs(ev.n, &ev.sort_len);
     ev.sort_first = (int32_t)std::min<int64_t>(warps, INT32_MAX);
     ev.sort_base = (int32_t)std::min<int64_t>(entries, INT32_MAX);
     warps += ev.sort_chunks;
     entries += T * ev.sort_chunks;
     max_tiles = (int32_t)std::max<int64_t>(max_tiles, std::min<int64_t>(T, INT32_MAX));
   }
-  sh->stable = max_tiles <= kStableMaxTiles && entries <= N && warps < INT32_MAX;
+  sh->stable = max_tiles <= kStableMaxTiles && entries <= 4 * N && warps < INT32_MAX;
   sh->sort_warps = (int32_t)std::min<int64_t>(warps, INT32_MAX);
   sh->sort_entries = entries;
   sh->max_event_tiles = max_tiles;
@@ -226,6 +224,7 @@ size_t place(DeviceBuffers* b, const Capacity& c, char* base) {
   CLUE_PLACE(large_tiles, int32_t, N / 256 + 1);
   CLUE_PLACE(oversize, int32_t, N / 4096 + 1);
   CLUE_PLACE(status, uint32_t, 1);
+  CLUE_PLACE(stats, unsigned long long, 8);
   CLUE_PLACE(sorted_sigma, float, c.sigma ? D * N : 0);
   CLUE_PLACE(sorted_unc, float, c.unc ? N : 0);
   CLUE_PLACE(sorted_tag, uint32_t, c.tags ? N : 0);
@@ -639,6 +638,7 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
     io.point_base = piece->point_base;
     io.event_base = piece->event_base;
   }
+  io.stats = ws->profiling && !piece ? ws->b.stats : nullptr;
   const RunParams prm = make_run_params(params, pts, ws->tuning);
   reset_launch_count();
   if (use_graph && (e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
@@ -1191,6 +1191,25 @@ clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t
     if (e != cudaSuccess)
       return fail_cuda(e, "cudaEventElapsedTime");
   }
+  return CLUE_OK;
+}
+
+clue_status clue_workspace_sweep_stats(clue_workspace* ws, int64_t* stats, int32_t capacity) {
+  if (!ws || !stats)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "null argument");
+  if (!ws->profiling)
+    return fail(CLUE_ERR_RUNTIME, "profiling is not enabled on this workspace");
+  if (!ws->has_run)
+    return fail(CLUE_ERR_RUNTIME, "no run on this workspace yet");
+  clue_status s = wait_run(ws);
+  if (s != CLUE_OK)
+    return s;
+  unsigned long long v[8] = {};
+  cudaError_t e = cudaMemcpy(v, ws->b.stats, sizeof v, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess)
+    return fail_cuda(e, "statistics copy");
+  for (int i = 0; i < CLUE_N_SWEEP_STATS && i < capacity; ++i)
+    stats[i] = (int64_t)v[i];
   return CLUE_OK;
 }
 

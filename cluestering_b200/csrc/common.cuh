@@ -45,7 +45,8 @@ struct EventDesc {
   int32_t grid;       // index into the grid table
   // Stable tile binning: the event's points form sort_chunks runs of sort_len
   // consecutive points, run c binned by warp sort_first + c; its count matrix
-  // (tiles x runs, tile-major) starts at entry sort_base.
+  // (runs x tiles, run-major: run c's counts are contiguous) starts at entry
+  // sort_base.
   int32_t sort_first;
   int32_t sort_chunks;
   int32_t sort_len;
@@ -53,8 +54,10 @@ struct EventDesc {
 };
 
 // Tiles of one event the stable binning handles: each warp keeps a counter per
-// tile of its event in shared memory (48 KB per block at most).
-constexpr int kStableMaxTiles = 12288;
+// tile of its event in shared memory (16 KB).
+constexpr int kStableMaxTiles = 4096;
+// Points per run of the stable binning (one warp, 32 rounds).
+constexpr int kStableRun = 1024;
 
 // A run of consecutive points of one event, processed by one block.
 struct Chunk {

@@ -68,6 +68,7 @@ struct DeviceBuffers {
   int32_t* large_tiles = nullptr;  // tiles too large for the per-warp sort
   int32_t* oversize = nullptr;     // tiles needing a chunk merge
   uint32_t* status = nullptr;
+  unsigned long long* stats = nullptr;  // sweep statistics of a profiled run (8 counters)
   // staged inputs/outputs for the host entry points
   float* in_coords = nullptr;
   float* in_weight = nullptr;
@@ -97,17 +98,17 @@ struct RunShape {
   int32_t n_chunks = 0;
   // Stable tile binning (one warp per run of consecutive points of an event):
   // usable when every event has at most kStableMaxTiles tiles and the count
-  // matrices of all events hold at most n entries.
+  // matrices of all events hold at most 4 n entries (they live in the
+  // nearest-higher records, 16 bytes per point, free until the sweeps).
   bool stable = false;
   int32_t sort_warps = 0;
   int64_t sort_entries = 0;
   int32_t max_event_tiles = 0;
 };
 
-// Runs of the stable binning for an event of n points in T tiles: as many as
-// keep the event's count matrix (T x runs) within n entries, at most one per
-// 1,024 points, at least one. Returns the run count; *len = points per run.
-int32_t sort_runs(int64_t n, int64_t T, int32_t* len);
+// Runs of the stable binning for an event of n points: one per kStableRun
+// points, at least one. Returns the run count; *len = points per run.
+int32_t sort_runs(int64_t n, int32_t* len);
 
 // Pointers of one run's inputs and outputs (device memory).
 struct RunIO {
@@ -128,6 +129,9 @@ struct RunIO {
   int32_t* piece_base = nullptr;
   int64_t point_base = 0;
   int32_t event_base = 0;
+  // Sweep statistics: when set, the run zeroes these 8 counters and the sweeps
+  // add to them (see SweepArgs::stats).
+  unsigned long long* stats = nullptr;
 };
 
 // Host tables built for a run.

@@ -183,12 +183,12 @@ __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, cons
 // ---------------------------------------------------------------------------
 // Stable tile binning: one warp per run of consecutive points of one event,
 // runs of an event in index order. Binning counts each run's points per tile
-// into the event's count matrix (tiles x runs, tile-major); an exclusive scan
-// of all matrices turns every entry into the sorted position of that run's
-// first point in that tile; the scatter then places each run's points in
-// index order from those positions. Every tile thus lists its points in
-// ascending index, the order the reference's serial fill produces
-// (data_structures/detail/AssociationMap.hpp:63-81), with no sort.
+// into the event's count matrix (runs x tiles, run-major); a pass per tile
+// turns its column into exclusive prefixes over the runs and the tile's
+// total; a scan of the totals gives the tile offsets; the scatter then places
+// each run's points in index order from offset + prefix. Every tile thus
+// lists its points in ascending index, the order the reference's serial fill
+// produces (data_structures/detail/AssociationMap.hpp:63-81), with no sort.
 // ---------------------------------------------------------------------------
 
 // Event of stable-binning warp w: the last event whose first warp is <= w.
@@ -262,8 +262,9 @@ __global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs 
       col[t] += __popc(mask);
     __syncwarp();  // the next round's leaders read these counters
   }
+  int32_t* row = matrix + (int64_t)ev.sort_base + (int64_t)c * T;
   for (int t = lane; t < T; t += 32)
-    matrix[(int64_t)ev.sort_base + (int64_t)t * ev.sort_chunks + c] = col[t];
+    row[t] = col[t];
   if (bounds) {
     lsb = __reduce_min_sync(kFull, lsb);
     vb = __reduce_max_sync(kFull, vb);
@@ -280,16 +281,49 @@ __global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs 
   }
 }
 
-// Places each run's points from its scanned matrix column. The first run of
-// each event also writes the event's tile offsets and lists its tiles of more
-// than kLargeTilePoints points (for k_cells).
+// Event of global tile g: the last event whose first tile is <= g.
+__device__ __forceinline__ int tile_event_of(const EventDesc* events, int n_events, int64_t g) {
+  int lo = 0, hi = n_events - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (events[mid].tile_base <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// One thread per tile: the tile's counts over the runs of its event become
+// exclusive prefixes (in place), and the total goes to tile_count. Threads of
+// consecutive tiles read consecutive entries of each run's row.
+__global__ void __launch_bounds__(kThreads) k_tile_prefix(const EventDesc* events, int n_events,
+                                                          const GridDesc* grids, int64_t n_tiles,
+                                                          int32_t* matrix, int32_t* tile_count) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_tiles;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const EventDesc ev = events[tile_event_of(events, n_events, g)];
+    const int64_t T = grids[ev.grid].T;
+    int32_t* m = matrix + (int64_t)ev.sort_base + (g - ev.tile_base);
+    int run = 0;
+    for (int c = 0; c < ev.sort_chunks; ++c) {
+      const int v = m[c * T];
+      m[c * T] = run;
+      run += v;
+    }
+    tile_count[g] = run;
+  }
+}
+
+// Places each run's points at tile offset + the run's prefix in that tile.
+// The first run of each event lists the event's tiles of more than
+// kLargeTilePoints points (for k_cells).
 __global__ void __launch_bounds__(kThreads) k_scatter_stable(const EventDesc* events, int n_events,
                                                              int n_warps, const GridDesc* grids,
                                                              const int32_t* tile_of, const int32_t* matrix,
-                                                             int max_tiles, int32_t* perm,
-                                                             int32_t* tile_offset, int64_t n_tiles,
-                                                             int32_t n_points, int32_t* large,
-                                                             int32_t* large_count) {
+                                                             int max_tiles, const int32_t* tile_offset,
+                                                             const int32_t* tile_count, int32_t* perm,
+                                                             int32_t* large, int32_t* large_count) {
   extern __shared__ int s_col[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -300,21 +334,13 @@ __global__ void __launch_bounds__(kThreads) k_scatter_stable(const EventDesc* ev
   const EventDesc ev = events[e];
   const int c = w - ev.sort_first;
   const int T = grids[ev.grid].T;
-  for (int t = lane; t < T; t += 32)
-    col[t] = matrix[(int64_t)ev.sort_base + (int64_t)t * ev.sort_chunks + c];
-  __syncwarp();
-  if (c == 0) {
-    for (int t = lane; t < T; t += 32) {
-      const int start = col[t];
-      tile_offset[ev.tile_base + t] = start;
-      const int next = t + 1 < T ? col[t + 1] : ev.begin + ev.n;
-      if (next - start > kLargeTilePoints)
-        large[atomicAdd(large_count, 1)] = ev.tile_base + t;
-    }
-    if (w == 0 && lane == 0)
-      tile_offset[n_tiles] = n_points;
-    __syncwarp();
+  const int32_t* row = matrix + (int64_t)ev.sort_base + (int64_t)c * T;
+  for (int t = lane; t < T; t += 32) {
+    col[t] = tile_offset[ev.tile_base + t] + row[t];
+    if (c == 0 && tile_count[ev.tile_base + t] > kLargeTilePoints)
+      large[atomicAdd(large_count, 1)] = ev.tile_base + t;
   }
+  __syncwarp();
   const int begin = ev.begin + c * ev.sort_len;
   const int end = min(ev.begin + ev.n, begin + ev.sort_len);
   for (int base = begin; base < end; base += 32) {
@@ -1069,6 +1095,8 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // grid extents
   CLUE_MARK(0);
+  if (io.stats)
+    CLUE_CHECK(fill32(io.stats, 16, 0, st));
   // exact-sum bounds per event (2-D and 3-D runs: their workspace holds them)
   int32_t* exact = (D == 2 || D == 3) ? b.event_exact : nullptr;
   const int64_t init_items = std::max<int64_t>((int64_t)sh.n_grids * kMaxDim, exact ? 4 * (int64_t)sh.n_events : 0);
@@ -1084,8 +1112,9 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   CLUE_MARK(1);
   if (sh.stable) {
     // Stable binning: runs of consecutive points, one warp each; the count
-    // matrices live in merge_tmp (at most n entries).
-    int32_t* matrix = b.merge_tmp;
+    // matrices (at most 4 n entries) live in the nearest-higher records, which
+    // the sweeps write much later.
+    int32_t* matrix = reinterpret_cast<int32_t*>(b.rec_nh);
     const int wpb = std::max(1, std::min(kThreads / 32, (48 << 10) / (4 * std::max(1, sh.max_event_tiles))));
     const int blocks = (sh.sort_warps + wpb - 1) / wpb;
     const size_t smem = (size_t)wpb * sh.max_event_tiles * sizeof(int);
@@ -1094,10 +1123,13 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
                                                  b.tile_of, b.point_event, matrix,
                                                  sh.max_event_tiles, io.weight, exact);
     CLUE_LAUNCHED();
-    CLUE_CHECK(scan(matrix, matrix, sh.sort_entries, b.counters + 7, b, st));
+    k_tile_prefix<<<grid_for(sh.n_tiles), kThreads, 0, st>>>(b.events, sh.n_events, b.grids, sh.n_tiles,
+                                                             matrix, b.tile_count);
+    CLUE_LAUNCHED();
+    CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));
     k_scatter_stable<<<blocks, wpb * 32, smem, st>>>(b.events, sh.n_events, sh.sort_warps, b.grids,
-                                                     b.tile_of, matrix, sh.max_event_tiles, b.perm,
-                                                     b.tile_offset, sh.n_tiles, (int32_t)n,
+                                                     b.tile_of, matrix, sh.max_event_tiles,
+                                                     b.tile_offset, b.tile_count, b.perm,
                                                      b.large_tiles, b.counters + 3);
     CLUE_LAUNCHED();
   } else {
@@ -1153,6 +1185,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.out_seed = io.is_seed;
   a.seed_flag = b.seed_flag;
   a.parent = b.parent;
+  a.stats = io.stats;
   if (sweep_fast_path(prm)) {
     a.nh_cells = sweep_cells_path(prm);
     a.nh_pos = b.nh_pos;

@@ -77,11 +77,11 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   sh.n_chunks = (int32_t)((n + kChunkPoints - 1) / kChunkPoints);
   // the one event and its stable-binning layout (as build_tables lays it out)
   EventDesc ev{0, (int32_t)n, 0, 0, 0, 0, 0, 0};
-  ev.sort_chunks = sort_runs(n, T, &ev.sort_len);
+  ev.sort_chunks = sort_runs(n, &ev.sort_len);
   sh.sort_warps = ev.sort_chunks;
   sh.sort_entries = T * (int64_t)ev.sort_chunks;
   sh.max_event_tiles = (int32_t)T;
-  sh.stable = T <= kStableMaxTiles && sh.sort_entries <= n;
+  sh.stable = T <= kStableMaxTiles && sh.sort_entries <= 4 * n;
 
   bool any_sigma = false;
   for (int d = 0; d < D; ++d)

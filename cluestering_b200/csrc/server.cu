@@ -721,10 +721,13 @@ clue_status clue_server_create(clue_server** out, const clue_server_config* cfg,
   srv->max_dim = max_dim;
   // Device bytes of one slot for batches of P points: workspace scratch (with
   // room for sigma, uncertainty and tags) plus the batch's input and output
-  // planes. The slots take at most half of the budget; the rest holds the
-  // resident events.
+  // planes. A batch size derived from the budget gives the slots at most half
+  // of it; a given one gives them what it needs. The rest of the budget holds
+  // the resident events.
   const int in_planes = 2 * max_dim + 3;
-  const int64_t per_slot = (int64_t)(cfg->budget_bytes / 2 / cfg->max_inflight);
+  const int64_t per_slot = cfg->max_batch_points > 0
+                               ? (int64_t)(cfg->budget_bytes / cfg->max_inflight)
+                               : (int64_t)(cfg->budget_bytes / 2 / cfg->max_inflight);
   auto slot_bytes = [&](int64_t P, int64_t E) {
     RunShape sh;
     sh.D = max_dim;
@@ -736,7 +739,7 @@ clue_status clue_server_create(clue_server** out, const clue_server_config* cfg,
     return (int64_t)scratch_bytes(sh, true, true, true) + P * (int64_t)(4 * (in_planes + 4));
   };
   int64_t P = cfg->max_batch_points > 0 ? cfg->max_batch_points : (int64_t)1 << 24;
-  while (P > 4096 && slot_bytes(P, cfg->max_batch_events) > per_slot)
+  while (cfg->max_batch_points <= 0 && P > 4096 && slot_bytes(P, cfg->max_batch_events) > per_slot)
     P /= 2;
   if (slot_bytes(P, cfg->max_batch_events) > per_slot) {
     delete srv;

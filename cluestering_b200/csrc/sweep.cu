@@ -681,7 +681,7 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
                               const GridDesc& g, const float* xi, int s, float wi, const int* inf,
                               const int* sup, bool ordered, const int* uinf, const int* usup,
                               float4 (*ring)[kChunk], int* off, int* qa, int* seg, int4* tinfo,
-                              float& rho) {
+                              float& rho, int& tested) {
   const int lane = threadIdx.x & 31;
   int nu[D];
   int64_t n_union = 1;
@@ -769,6 +769,7 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
       run += y;
   }
   const int total = __shfl_sync(kFullMask, run, 31);
+  tested = total;
   __syncwarp();
   if (2 * lane < K)
     off[2 * lane] = run - l0 - l1;
@@ -977,9 +978,10 @@ __global__ void __launch_bounds__(NT, MINB) k_density_fast(const RunParams p, co
     const bool exact = KIND == CLUE_KERNEL_FLAT && a.rec_cell != nullptr && one_grid && u_ordered &&
                        __all_sync(kFullMask, event_sums_exact(a.event_exact, a.sevt[s], ev.n));
     bool done = false;  // warp-uniform: the exact-sum path handled the warp
+    int tested = 0;     // candidate records this lane tests
     if (exact)
       done = density_exact<D>(p, a, ev, g, xi, s, wi, inf, sup, ordered, uinf, usup, ring, off, qa,
-                              s_seg[warp], s_tinfo[warp], rho);
+                              s_seg[warp], s_tinfo[warp], rho, tested);
     bool streamed = false;  // warp-uniform: the ordered stream handles the warp
     if (!done && one_grid && rows64 >= 1 && rows64 <= kMaxRows) {
       const int rows = (int)rows64;
@@ -1029,6 +1031,7 @@ __global__ void __launch_bounds__(NT, MINB) k_density_fast(const RunParams p, co
     if (streamed) {
       const int rows = (int)rows64;
       const int total = off[rows];
+      tested = total;
       // stream position of the point itself (its own tile is in the box unless
       // get_bin's clamping left it out)
       int p_self = -1;
@@ -1108,7 +1111,15 @@ __global__ void __launch_bounds__(NT, MINB) k_density_fast(const RunParams p, co
     if (!streamed && !done)
       for_each_candidate<D>(a, g, ev.tile_base, inf, sup, [&](int q) {
         density_add<D, KIND>(p, xi, __ldg(&rec[q]), q == s, wi, rho);
+        ++tested;
       });
+    if (a.stats) {  // warp-uniform
+      const int sum = __reduce_add_sync(kFullMask, active ? tested : 0);
+      if (lane == 0) {
+        atomicAdd(&a.stats[0], (unsigned long long)sum);
+        atomicAdd(&a.stats[1], 1ull);
+      }
+    }
     if (!active)
       continue;
     a.srho[s] = rho;
@@ -1513,9 +1524,11 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
 
 // Tests the members of one cell unless the cell is empty, holds no higher
 // key, or its box is out of reach.
+// `cnt` counts cells checked, cells entered and members tested (statistics).
 template <int D>
 __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const float* xi,
-                                           uint64_t key_i, float eff2, NhBest& st) {
+                                           uint64_t key_i, float eff2, NhBest& st, int* cnt) {
+  ++cnt[0];
   const CellInfo ci = a.cell_info[slot];
   if (ci.start == ci.end || ci.maxkey <= key_i)
     return;
@@ -1524,6 +1537,8 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
   const float lb2 = box_lower_bound<D>(xi, mn, mx);
   if (lb2 > eff2 || lb2 >= st.hi)
     return;
+  ++cnt[1];
+  cnt[2] += ci.end - ci.start;
   const float4* __restrict__ rec = a.rec_nh;
 #pragma unroll 4
   for (int q = ci.start; q < ci.end; ++q) {
@@ -1568,6 +1583,7 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
       continue;
     const int pi = a.walk[w];  // neighbouring points in neighbouring lanes
     const int s = a.nh_q[pi];
+    int cnt[3] = {0, 0, 0};  // cells checked, cells entered, members tested
     const float4 ri = rec[pi];
     const float xi[3] = {ri.x, ri.y, ri.z};
     const float zero[3] = {0.0f, 0.0f, 0.0f};
@@ -1645,7 +1661,7 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
             seen &= abs(cd - c0[d]) <= 1;
           }
           if (valid && !seen)
-            visit_cell<D>(a, base + lin, xi, key_i, eff2, bs);
+            visit_cell<D>(a, base + lin, xi, key_i, eff2, bs, cnt);
         } while (next_tile<D>(c, c_lo, c_hi));
       }
       if (first)
@@ -1654,6 +1670,17 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
         break;
     }
 
+    if (a.stats) {
+      const unsigned am = __activemask();
+      const int members = __reduce_add_sync(am, cnt[2]);
+      const int checked = __reduce_add_sync(am, cnt[0]);
+      const int entered = __reduce_add_sync(am, cnt[1]);
+      if (lane == __ffs(am) - 1) {
+        atomicAdd(&a.stats[2], (unsigned long long)members);
+        atomicAdd(&a.stats[3], (unsigned long long)checked);
+        atomicAdd(&a.stats[4], (unsigned long long)entered);
+      }
+    }
     const int gi = a.perm[s];
     const int qb = bs.best >= 0 ? a.nh_q[bs.best] : s;
     const int nh = bs.best >= 0 ? a.perm[qb] : -1;

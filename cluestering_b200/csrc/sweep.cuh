@@ -77,6 +77,10 @@ struct SweepArgs {
   float4* cell_geom;      // per tile: D = 2 {lo0, lo1, inv0, inv1}; D = 3 two entries
   CellInfo* cell_info;    // per slot
   float4* cell_box;       // per slot: bounding box of the members (D = 3: two entries)
+  // Sweep statistics (null unless the run counts them): [0] density candidate
+  // tests (a lane testing one record), [1] density work items, [2] nearest-
+  // higher members tested, [3] cells checked, [4] cells whose members were tested.
+  unsigned long long* stats;
 };
 
 // True when the packed fast path applies: D = 2 or 3, Euclidean metric, no

@@ -150,6 +150,15 @@ size_t clue_workspace_bytes_for(int32_t ndim, int64_t n_points, int64_t n_tiles,
 #define CLUE_N_STAGES 6
 clue_status clue_workspace_set_profiling(clue_workspace* ws, int32_t enable);
 clue_status clue_workspace_stage_ms(clue_workspace* ws, float* stage_ms, int32_t capacity);
+/* Sweep statistics of the last profiled run (device counters the sweeps add to
+ * while profiling is on; no reference counterpart): [0] density candidate
+ * tests (one point tested against one candidate record), [1] density work
+ * items of 32 points, [2] nearest-higher candidate members tested, [3] cells
+ * checked by the nearest-higher search, [4] cells whose members it tested.
+ * The nearest-higher counters cover the cell search (2-D and 3-D Euclidean runs
+ * without user tags); other paths leave them at 0. Waits for the run. */
+#define CLUE_N_SWEEP_STATS 5
+clue_status clue_workspace_sweep_stats(clue_workspace* ws, int64_t* stats, int32_t capacity);
 /* CUDA-graph replay (off by default; no reference counterpart). When on, a
  * device run on a non-default stream (without stage timing) is captured into a
  * CUDA graph, and a later run with identical arguments — the same pointers,
@@ -366,8 +375,9 @@ typedef struct {
 typedef struct {
   int32_t device;
   /* Device memory the server may hold: the stream slots (each a workspace and
-   * the planes of one batch, together at most half of it) and the resident
-   * pool of admitted events (the rest). */
+   * the planes of one batch) and the resident pool of admitted events (the
+   * rest, at least one batch of event planes). When max_batch_points is 0 the
+   * batch size is chosen so that the slots take at most half of it. */
   size_t budget_bytes;
   int32_t max_inflight;     /* batches on the GPU at once (one stream slot each) */
   int32_t max_batch_events; /* events per batch */

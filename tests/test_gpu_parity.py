@@ -608,3 +608,22 @@ def test_graph_replay_reads_new_contents_and_recaptures_on_new_shapes():
     c.set_graphs(False)
     c.make_clusters(pts, batch_item_sizes=sizes2, grid_mode=clue.GRID_PER_EVENT, stream=stream)
     assert not c.graph_replayed()
+
+
+def test_sweep_statistics_of_a_profiled_run():
+    # Profiling counts the sweeps' candidate tests without changing a result.
+    ev = W.single_2d()
+    c = clue.Clusterer(1.5, 5.0, 1.5)
+    c.set_profiling(True)
+    g, o = check(ev.coords, ev.weights, 1.5, 5.0, 1.5, clusterer=c, path="device")
+    st = c.sweep_stats()
+    assert st["density_items"] == (ev.n + 31) // 32
+    # every point tests at least the candidates in range of it (unit weights:
+    # rho = 1 + 0.5 (in range - 1))
+    in_range = int((2.0 * (o.rho.astype(np.float64) - 1.0) + 1.0).sum())
+    assert st["density_tests"] >= in_range > 0
+    assert st["nh_cells_checked"] >= st["nh_cells_entered"] > 0
+    assert st["nh_members_tested"] > 0
+    c.set_profiling(False)
+    with pytest.raises(RuntimeError):
+        c.sweep_stats()

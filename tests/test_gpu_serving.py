@@ -191,16 +191,20 @@ def test_admission_by_device_memory_budget():
     # with the single-event result.
     evs = _events(50, seed=43)
     pts = [_host_points(ev, pinned=True) for _, ev in evs]
-    with clue.Server([P2, P3], max_inflight=2, max_batch_events=4, max_batch_points=65536,
-                     budget_bytes=96 << 20) as srv:
+    cfg = dict(max_inflight=2, max_batch_events=4, max_batch_points=65536)
+    with clue.Server([P2, P3], budget_bytes=1 << 30, **cfg) as srv:
+        slots = srv.stats()["slot_bytes"]
+    budget = slots + (3 << 20)  # the slots, and a pool of 3 MiB for the events' points
+    with clue.Server([P2, P3], budget_bytes=budget, **cfg) as srv:
         for (prof, _), p in zip(evs, pts):
             srv.submit(prof, p)
         srv.drain()
         st = srv.stats()
     assert st["completed"] == len(evs)
+    assert sum(ev.n * 4 * (ev.ndim + 1) for _, ev in evs) > 3 << 20
     assert st["admission_waits"] > 0
     assert 0 < st["resident_bytes_peak"] <= st["resident_pool_bytes"]
-    assert st["slot_bytes"] + st["resident_pool_bytes"] <= 96 << 20
+    assert st["slot_bytes"] + st["resident_pool_bytes"] <= budget
     for (prof, ev), p in zip(evs, pts):
         a = _alone(prof, ev)
         assert np.array_equal(p.cluster_index, a.cluster_index)
