@@ -319,6 +319,7 @@ enum : uint32_t {
   kStatusScanTimeout = 1u << 0,
   kStatusSortOverflow = 1u << 1,
   kStatusLabelTimeout = 1u << 2,
+  kStatusCopyTimeout = 1u << 3,
 };
 
 }  // namespace clue_impl

@@ -1186,6 +1186,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   a.seed_flag = b.seed_flag;
   a.parent = b.parent;
   a.stats = io.stats;
+  a.status = b.status;
   if (sweep_fast_path(prm)) {
     a.nh_cells = sweep_cells_path(prm);
     a.nh_pos = b.nh_pos;

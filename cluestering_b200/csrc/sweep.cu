@@ -527,6 +527,57 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Bulk copies (the copy engine inside each SM) into this CTA's shared memory,
+// completed on an mbarrier by transaction bytes. Sources are this GPU's own
+// memory; nothing is multicast.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Orders this thread's earlier shared-memory accesses before later bulk copies
+// into the same buffer.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// dst and src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase of `bar` with this parity, at most kCopyWaitLimit polls
+// (each poll itself bounded by the hardware's try-wait time limit). On giving
+// up it records kStatusCopyTimeout, so the host call reports CLUE_ERR_TIMEOUT.
+constexpr int kCopyWaitLimit = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, uint32_t* status) {
+  for (int it = 0; it < kCopyWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity))
+      return true;
+  atomicOr(status, kStatusCopyTimeout);
+  return false;
+}
+
 // Contribution of candidate record r (sorted position q) to rho_i.
 template <int D, int KIND>
 __device__ __forceinline__ void density_add(const RunParams& p, const float* xi, const float4& r,

@@ -81,6 +81,8 @@ struct SweepArgs {
   // tests (a lane testing one record), [1] density work items, [2] nearest-
   // higher members tested, [3] cells checked, [4] cells whose members were tested.
   unsigned long long* stats;
+  // Status word of the run: kernels with bounded waits set bits here.
+  uint32_t* status;
 };
 
 // True when the packed fast path applies: D = 2 or 3, Euclidean metric, no
