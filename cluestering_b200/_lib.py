@@ -63,7 +63,7 @@ class Points(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("density_union_x16_2d", C.c_int32), ("density_union_x16_3d", C.c_int32),
                 ("label_jump_rounds", C.c_int32), ("cell_points", C.c_int32),
-                ("density_shape", C.c_int32), ("nh_shape", C.c_int32)]
+                ("density_shape", C.c_int32), ("nh_shape", C.c_int32), ("tile_binning", C.c_int32)]
 
 
 class ServerProfile(C.Structure):

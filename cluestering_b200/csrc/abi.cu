@@ -405,6 +405,7 @@ clue_tuning default_tuning() {
   t.cell_points = 2;
   t.density_shape = 0;
   t.nh_shape = 0;
+  t.tile_binning = 1;
   return t;
 }
 
@@ -415,6 +416,7 @@ RunParams make_run_params(const clue_params* p, const clue_points* pts, const cl
   r.cell_points = t.cell_points;
   r.dens_shape = t.density_shape;
   r.nh_shape = t.nh_shape;
+  r.stable_binning = t.tile_binning;
   r.D = pts->ndim;
   r.dc = p->dc;
   r.rhoc = p->rhoc;
@@ -1106,6 +1108,8 @@ clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tun
   if (tuning->density_shape < 0 || tuning->density_shape > 2 || tuning->nh_shape < 0 ||
       tuning->nh_shape > 2)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "density_shape and nh_shape must be in [0, 2]");
+  if (tuning->tile_binning < 0 || tuning->tile_binning > 1)
+    return fail(CLUE_ERR_INVALID_ARGUMENT, "tile_binning must be 0 or 1");
   ws->tuning = *tuning;
   return CLUE_OK;
 }
@@ -1332,6 +1336,7 @@ clue_status clue_workspace_autotune(clue_workspace* ws, const clue_params* param
     try_field(&clue_tuning::density_shape, {0, 1, 2});
     try_field(&clue_tuning::nh_shape, {0, 1, 2});
   }
+  try_field(&clue_tuning::tile_binning, {0, 1});
   try_field(&clue_tuning::label_jump_rounds, {0, 1, 2, 3, 4});
   for (auto& x : ev)
     cudaEventDestroy(x);

@@ -109,6 +109,8 @@ struct RunParams {
   // (clue_tuning::density_shape, nh_shape).
   int32_t dens_shape;
   int32_t nh_shape;
+  // Stable tile binning when the run's shape allows it (clue_tuning::tile_binning).
+  int32_t stable_binning;
 };
 
 // ---------------------------------------------------------------------------

@@ -132,6 +132,9 @@ __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, cons
     sg = grids[ev.grid];
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  const bool bounds = event_exact && p.kernel_kind == CLUE_KERNEL_FLAT;  // block-uniform
+  int lsb = INT_MAX, bad = 0;
+  uint32_t vb = 0, wb = 0;
   for (int base = c.begin; base < c.end; base += blockDim.x) {
     const int i = base + threadIdx.x;
     const bool valid = i < c.end;
@@ -143,39 +146,52 @@ __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, cons
       t = b;
       tile_of[i] = t;
       point_event[i] = c.event;
+      if (bounds) {
+        const float w = weight[i];
+        const float v = __fmul_rn(p.kernel_p0, w);  // a neighbour's fl(flat * w_j)
+        const int bd = !(w >= 0.0f) || signbit(w) || isinf(w) || isinf(v);
+        bad |= bd;
+        if (!bd) {
+          if (v > 0.0f)
+            lsb = min(lsb, lsb_exponent(v));
+          if (w > 0.0f)
+            lsb = min(lsb, lsb_exponent(w));
+          vb = max(vb, __float_as_uint(v));
+          wb = max(wb, __float_as_uint(w));
+        }
+      }
     }
     const unsigned mask = __match_any_sync(kFull, t);
     const int leader = __ffs(mask) - 1;
     if (valid && lane == leader)
       atomicAdd(&tile_count[t], __popc(mask));
-    if (event_exact && p.kernel_kind == CLUE_KERNEL_FLAT) {  // block-uniform
-      int lsb = INT_MAX, bad = 0;
-      uint32_t vb = 0, wb = 0;
-      if (valid) {
-        const float w = weight[i];
-        const float v = __fmul_rn(p.kernel_p0, w);  // a neighbour's fl(flat * w_j)
-        bad = !(w >= 0.0f) || signbit(w) || isinf(w) || isinf(v);
-        if (!bad) {
-          if (v > 0.0f)
-            lsb = min(lsb, lsb_exponent(v));
-          if (w > 0.0f)
-            lsb = min(lsb, lsb_exponent(w));
-          vb = __float_as_uint(v);
-          wb = __float_as_uint(w);
-        }
-      }
-      lsb = __reduce_min_sync(kFull, lsb);
-      vb = __reduce_max_sync(kFull, vb);
-      wb = __reduce_max_sync(kFull, wb);
-      bad = __any_sync(kFull, bad);
-      if (lane == 0) {
-        int32_t* st = event_exact + 4 * c.event;
-        atomicMin(&st[0], lsb);
-        atomicMax(reinterpret_cast<unsigned*>(&st[1]), vb);
-        atomicMax(reinterpret_cast<unsigned*>(&st[2]), wb);
-        if (bad)
-          atomicOr(&st[3], 1);
-      }
+  }
+  // the chunk's bounds, one set of atomics per block
+  if (bounds) {
+    __shared__ int s_b[4];
+    if (threadIdx.x == 0) {
+      s_b[0] = INT_MAX;
+      s_b[1] = s_b[2] = s_b[3] = 0;
+    }
+    __syncthreads();
+    lsb = __reduce_min_sync(kFull, lsb);
+    vb = __reduce_max_sync(kFull, vb);
+    wb = __reduce_max_sync(kFull, wb);
+    bad = __any_sync(kFull, bad);
+    if (lane == 0) {
+      atomicMin(&s_b[0], lsb);
+      atomicMax(reinterpret_cast<unsigned*>(&s_b[1]), vb);
+      atomicMax(reinterpret_cast<unsigned*>(&s_b[2]), wb);
+      atomicOr(&s_b[3], bad);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int32_t* st = event_exact + 4 * c.event;
+      atomicMin(&st[0], s_b[0]);
+      atomicMax(reinterpret_cast<unsigned*>(&st[1]), (unsigned)s_b[1]);
+      atomicMax(reinterpret_cast<unsigned*>(&st[2]), (unsigned)s_b[2]);
+      if (s_b[3])
+        atomicOr(&st[3], 1);
     }
   }
 }
@@ -211,7 +227,8 @@ __global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs 
                                                          int n_events, int n_warps, const GridDesc* grids,
                                                          int32_t* tile_of, int32_t* point_event,
                                                          int32_t* matrix, int max_tiles,
-                                                         const float* weight, int32_t* event_exact) {
+                                                         const float* weight, int32_t* event_exact,
+                                                         int32_t* tile_event) {
   extern __shared__ int s_col[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -231,6 +248,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs 
   const bool bounds = event_exact && p.kernel_kind == CLUE_KERNEL_FLAT;
   int lsb = INT_MAX, bad = 0;
   uint32_t vb = 0, wb = 0;
+#pragma unroll 4
   for (int base = begin; base < end; base += 32) {
     const int i = base + lane;
     const bool valid = i < end;
@@ -259,10 +277,13 @@ __global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs 
     }
     const unsigned mask = __match_any_sync(kFull, t);
     if (valid && lane == __ffs(mask) - 1)
-      col[t] += __popc(mask);
-    __syncwarp();  // the next round's leaders read these counters
+      atomicAdd(&col[t], __popc(mask));  // ordered with later rounds' leaders, no barrier
   }
+  __syncwarp();
   int32_t* row = matrix + (int64_t)ev.sort_base + (int64_t)c * T;
+  if (c == 0)  // the event of each of its tiles, for the prefix pass
+    for (int t = lane; t < T; t += 32)
+      tile_event[ev.tile_base + t] = e;
   for (int t = lane; t < T; t += 32)
     row[t] = col[t];
   if (bounds) {
@@ -281,31 +302,19 @@ __global__ void __launch_bounds__(kThreads) k_bin_stable(RunParams p, CoordPtrs 
   }
 }
 
-// Event of global tile g: the last event whose first tile is <= g.
-__device__ __forceinline__ int tile_event_of(const EventDesc* events, int n_events, int64_t g) {
-  int lo = 0, hi = n_events - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (events[mid].tile_base <= g)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
-
 // One thread per tile: the tile's counts over the runs of its event become
 // exclusive prefixes (in place), and the total goes to tile_count. Threads of
 // consecutive tiles read consecutive entries of each run's row.
-__global__ void __launch_bounds__(kThreads) k_tile_prefix(const EventDesc* events, int n_events,
-                                                          const GridDesc* grids, int64_t n_tiles,
+__global__ void __launch_bounds__(kThreads) k_tile_prefix(const EventDesc* events, const GridDesc* grids,
+                                                          int64_t n_tiles, const int32_t* tile_event,
                                                           int32_t* matrix, int32_t* tile_count) {
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_tiles;
        g += (int64_t)gridDim.x * blockDim.x) {
-    const EventDesc ev = events[tile_event_of(events, n_events, g)];
+    const EventDesc ev = events[tile_event[g]];
     const int64_t T = grids[ev.grid].T;
     int32_t* m = matrix + (int64_t)ev.sort_base + (g - ev.tile_base);
     int run = 0;
+#pragma unroll 8
     for (int c = 0; c < ev.sort_chunks; ++c) {
       const int v = m[c * T];
       m[c * T] = run;
@@ -343,10 +352,14 @@ __global__ void __launch_bounds__(kThreads) k_scatter_stable(const EventDesc* ev
   __syncwarp();
   const int begin = ev.begin + c * ev.sort_len;
   const int end = min(ev.begin + ev.n, begin + ev.sort_len);
+  // Rounds of 32 points in index order; the next round's tile ids are loaded
+  // before this round's cursor updates, so the load latency overlaps them.
+  int t_next = begin + lane < end ? tile_of[begin + lane] - ev.tile_base : -1;
   for (int base = begin; base < end; base += 32) {
     const int i = base + lane;
     const bool valid = i < end;
-    const int t = valid ? tile_of[i] - ev.tile_base : -1;
+    const int t = t_next;
+    t_next = base + 32 + lane < end ? tile_of[base + 32 + lane] - ev.tile_base : -1;
     const unsigned mask = __match_any_sync(kFull, t);
     const int leader = __ffs(mask) - 1;
     int pos = 0;
@@ -1110,7 +1123,7 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // counting sort by tile
   CLUE_MARK(1);
-  if (sh.stable) {
+  if (sh.stable && prm.stable_binning) {
     // Stable binning: runs of consecutive points, one warp each; the count
     // matrices (at most 4 n entries) live in the nearest-higher records, which
     // the sweeps write much later.
@@ -1121,9 +1134,9 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     CLUE_CHECK(fill32(b.counters + 3, 1, 0, st));  // large-tile count
     k_bin_stable<<<blocks, wpb * 32, smem, st>>>(prm, x, b.events, sh.n_events, sh.sort_warps, b.grids,
                                                  b.tile_of, b.point_event, matrix,
-                                                 sh.max_event_tiles, io.weight, exact);
+                                                 sh.max_event_tiles, io.weight, exact, b.tile_cursor);
     CLUE_LAUNCHED();
-    k_tile_prefix<<<grid_for(sh.n_tiles), kThreads, 0, st>>>(b.events, sh.n_events, b.grids, sh.n_tiles,
+    k_tile_prefix<<<grid_for(sh.n_tiles), kThreads, 0, st>>>(b.events, b.grids, sh.n_tiles, b.tile_cursor,
                                                              matrix, b.tile_count);
     CLUE_LAUNCHED();
     CLUE_CHECK(scan(b.tile_count, b.tile_offset, sh.n_tiles, b.tile_offset + sh.n_tiles, b, st));

@@ -1575,6 +1575,23 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
 
 // Tests the members of one cell unless the cell is empty, holds no higher
 // key, or its box is out of reach.
+// Bounds on the bin of any coordinate >= c (bin_below) or <= c (bin_above),
+// for a grid without wrapping: get_bin's expression, with the cases where its
+// x86 conversion is not monotone (infinite or NaN quotients, which only a zero
+// tile size or an enormous coordinate give) sent to the widest bound.
+__device__ __forceinline__ int bin_below(const GridDesc& g, float c, int d) {
+  const float u = __fdiv_rn(__fsub_rn(c, g.minv[d]), g.tile[d]);
+  if (!(u < 2147483648.0f))  // NaN or >= 2^31
+    return u == u ? g.k - 1 : 0;
+  return u < 0.0f ? 0 : min((int)u, g.k - 1);
+}
+__device__ __forceinline__ int bin_above(const GridDesc& g, float c, int d) {
+  const float u = __fdiv_rn(__fsub_rn(c, g.minv[d]), g.tile[d]);
+  if (!(u < 2147483648.0f))  // NaN or >= 2^31
+    return g.k - 1;
+  return u < 0.0f ? 0 : min((int)u, g.k - 1);
+}
+
 // `cnt` counts cells checked, cells entered and members tested (statistics).
 template <int D>
 __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const float* xi,
@@ -1715,10 +1732,25 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
             visit_cell<D>(a, base + lin, xi, key_i, eff2, bs, cnt);
         } while (next_tile<D>(c, c_lo, c_hi));
       }
-      if (first)
+      if (first) {
+        // Phase 1 visits only the tiles of the box that can hold a point
+        // within reach of the best so far (every point that can still win has
+        // each coordinate within R of the point's, and bins are monotone).
         first = false;
-      else if (!next_tile<D>(b, inf, sup))
+        const float R = reach(fminf(eff2, bs.hi));
+        bool empty = false;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          inf[d] = max(inf[d], bin_below(g, __fsub_rd(xi[d], R), d));
+          sup[d] = min(sup[d], bin_above(g, __fadd_ru(xi[d], R), d));
+          b[d] = inf[d];
+          empty |= inf[d] > sup[d];
+        }
+        if (empty)
+          break;
+      } else if (!next_tile<D>(b, inf, sup)) {
         break;
+      }
     }
 
     if (a.stats) {

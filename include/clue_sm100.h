@@ -214,6 +214,12 @@ typedef struct {
    * blocks per SM in 2-D (4 in 3-D), 1 = 256 threads with 6, 2 = 128 threads
    * with 16 in 2-D (8 in 3-D). */
   int32_t nh_shape;
+  /* Tile binning: 0 = counting sort by atomics, then each tile's points put
+   * in ascending index; 1 = stable runs (one warp per run of consecutive
+   * points, per-event count matrices), used when every event of the run has at
+   * most 4,096 tiles (else 0). Both give every tile its points in ascending
+   * index. */
+  int32_t tile_binning;
 } clue_tuning;
 
 /* Defaults: the values the library ships with. */
@@ -221,7 +227,8 @@ clue_status clue_tuning_defaults(clue_tuning* out);
 /* The workspace's current choices (defaults until set or autotuned). */
 clue_status clue_workspace_get_tuning(const clue_workspace* ws, clue_tuning* out);
 /* CLUE_ERR_INVALID_ARGUMENT if a field is out of range (a negative threshold,
- * jump rounds outside -1..4, cell_points outside 1..8, a shape outside 0..2). */
+ * jump rounds outside -1..4, cell_points outside 1..8, a shape outside 0..2,
+ * tile_binning outside 0..1). */
 clue_status clue_workspace_set_tuning(clue_workspace* ws, const clue_tuning* tuning);
 /* Autotuner: runs make_clusters on these device points (the single-event form
  * when event_sizes is NULL, else the batched form with grid_mode) under

@@ -125,8 +125,8 @@ def test_tuning_defaults_and_struct_layout():
     # 2-D mixed warps stream unions up to 1.25x; 3-D always streams; jump rounds by size
     assert (t.density_union_x16_2d, t.density_union_x16_3d, t.label_jump_rounds) == (20, 1 << 20, -1)
     # two points per cell on average, the default block shapes of both sweeps
-    assert (t.cell_points, t.density_shape, t.nh_shape) == (2, 0, 0)
-    assert C.sizeof(L.Tuning) == 24
+    assert (t.cell_points, t.density_shape, t.nh_shape, t.tile_binning) == (2, 0, 0, 1)
+    assert C.sizeof(L.Tuning) == 28
     assert L.load().clue_tuning_defaults(None) == L.ERR_INVALID_ARGUMENT
 
 

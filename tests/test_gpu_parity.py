@@ -489,11 +489,11 @@ def test_small_host_batch_runs_in_one_piece():
 
 TUNINGS = [
     dict(density_union_x16_2d=0, density_union_x16_3d=0, label_jump_rounds=0, cell_points=1,
-         density_shape=1, nh_shape=2),
+         density_shape=1, nh_shape=2, tile_binning=0),
     dict(density_union_x16_2d=1 << 20, density_union_x16_3d=1 << 20, label_jump_rounds=4, cell_points=8,
-         density_shape=2, nh_shape=1),
+         density_shape=2, nh_shape=1, tile_binning=1),
     dict(density_union_x16_2d=16, density_union_x16_3d=24, label_jump_rounds=1, cell_points=3,
-         density_shape=0, nh_shape=0),
+         density_shape=0, nh_shape=0, tile_binning=0),
 ]
 
 
@@ -539,6 +539,8 @@ def test_set_tuning_rejects_out_of_range():
         c.set_tuning(density_shape=3)
     with pytest.raises(ValueError):
         c.set_tuning(nh_shape=-1)
+    with pytest.raises(ValueError):
+        c.set_tuning(tile_binning=2)
     with pytest.raises(KeyError):
         c.set_tuning(points_per_tile=64)
 
