@@ -1592,11 +1592,15 @@ __device__ __forceinline__ int bin_above(const GridDesc& g, float c, int d) {
   return u < 0.0f ? 0 : min((int)u, g.k - 1);
 }
 
+// Whether the warp runs phase 0 of the cell search as one shared stream.
+constexpr bool kCoopPhase0 = true;
+
 // `cnt` counts cells checked, cells entered and members tested (statistics).
-template <int D>
+template <int D, bool STATS>
 __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const float* xi,
                                            uint64_t key_i, float eff2, NhBest& st, int* cnt) {
-  ++cnt[0];
+  if (STATS)
+    ++cnt[0];
   const CellInfo ci = a.cell_info[slot];
   if (ci.start == ci.end || ci.maxkey <= key_i)
     return;
@@ -1605,8 +1609,10 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
   const float lb2 = box_lower_bound<D>(xi, mn, mx);
   if (lb2 > eff2 || lb2 >= st.hi)
     return;
-  ++cnt[1];
-  cnt[2] += ci.end - ci.start;
+  if (STATS) {
+    ++cnt[1];
+    cnt[2] += ci.end - ci.start;
+  }
   const float4* __restrict__ rec = a.rec_nh;
 #pragma unroll 4
   for (int q = ci.start; q < ci.end; ++q) {
@@ -1631,7 +1637,9 @@ __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const f
 // 256 threads per SM measured 8.3 ms on the 46.5 M-point batch against 9.4 ms
 // at 5 and 10.8 ms at 4, small spills included. The 3-D form, with more state
 // per lane, stays at 4.
-template <int D, int NT, int MINB>
+// STATS: the profiling instantiation, which also counts the candidates tested
+// (SweepArgs::stats); the counters cost registers, so timed runs go without.
+template <int D, int NT, int MINB, bool STATS>
 __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunParams p, const SweepArgs a) {
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_nh;
@@ -1647,9 +1655,10 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
     if (item >= n_items)
       break;
     const int64_t w = item * 32 + lane;
-    if (w >= n)
-      continue;
-    const int pi = a.walk[w];  // neighbouring points in neighbouring lanes
+    // lanes past the end shadow lane 0 (the warp-wide steps below need every
+    // lane) and write nothing
+    const bool active = w < n;
+    const int pi = a.walk[active ? w : item * 32];  // neighbouring points in neighbouring lanes
     const int s = a.nh_q[pi];
     int cnt[3] = {0, 0, 0};  // cells checked, cells entered, members tested
     const float4 ri = rec[pi];
@@ -1683,14 +1692,89 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
     // coordinate beyond the int range to bin 0 (x86 conversion), so a huge
     // radius can give a box that misses the point's own tile.
     int c0[D], b[D];
+    int slo[D], shi[D];  // cells of the own tile that phase 0 searched
     bool first = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       b[d] = inf[d];
       c0[d] = 0;
+      slo[d] = 1;
+      shi[d] = 0;
       first &= inf[d] <= own[d] && own[d] <= sup[d];
     }
-    for (;;) {
+    // Phase 1 visits only the tiles of the box that can hold a point within
+    // reach of the best so far (every point that can still win has each
+    // coordinate within R of the point's, and bins are monotone).
+    auto prune_box = [&]() {
+      const float R = reach(fminf(eff2, bs.hi));
+      bool empty = false;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        inf[d] = max(inf[d], bin_below(g, __fsub_rd(xi[d], R), d));
+        sup[d] = min(sup[d], bin_above(g, __fadd_ru(xi[d], R), d));
+        b[d] = inf[d];
+        empty |= inf[d] > sup[d];
+      }
+      return !empty;
+    };
+    bool search = true;
+    if (kCoopPhase0) {
+      // Phase 0 shared by the warp: the lanes whose own tile is lane 0's
+      // (the home tile, in their boxes) stream together the members of the
+      // union of their own cells' neighbourhoods, every record read once for
+      // all of them; each lane tests it with its own key and bounds.
+      const int home = __shfl_sync(kFullMask, t0, 0);
+      const bool coop = first && t0 == home;
+      const int st_h = a.cell_s[home];
+      float glo[D], ginv[D];
+      load_geom<D>(a, home, glo, ginv);
+      int ulo[D], uhi[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int cc = cell_coord(xi[d], glo[d], ginv[d], st_h);
+        ulo[d] = max(__reduce_min_sync(kFullMask, coop ? cc : INT_MAX) - 1, 0);
+        uhi[d] = min(__reduce_max_sync(kFullMask, coop ? cc : INT_MIN) + 1, st_h - 1);
+      }
+      if (__any_sync(kFullMask, coop)) {  // warp-uniform
+        const int base_h = a.tile_offset[home];
+        const float thr = coop ? eff2 : -1.0f;  // other lanes take nothing here
+        int rows = uhi[0] - ulo[0] + 1;
+        if (D == 3)
+          rows *= uhi[1] - ulo[1] + 1;
+        for (int r = 0; r < rows; ++r) {
+          int row_cell;
+          if (D == 2) {
+            row_cell = (ulo[0] + r) * st_h;
+          } else {
+            const int n1 = uhi[1] - ulo[1] + 1;
+            row_cell = ((ulo[0] + r / n1) * st_h + ulo[1] + r % n1) * st_h;
+          }
+          const int q0 = a.cell_info[base_h + row_cell + ulo[D - 1]].start;
+          const int q1 = a.cell_info[base_h + row_cell + uhi[D - 1]].end;
+          if (STATS && coop)
+            cnt[2] += q1 - q0;
+#pragma unroll 4
+          for (int q = q0; q < q1; ++q) {
+            const float4 r4 = __ldg(&rec[q]);
+            const uint32_t tag_j = D == 2 ? __float_as_uint(r4.w) : __ldg(&a.rec_tag[q]);
+            const uint64_t key_j = ((uint64_t)__float_as_uint(D == 2 ? r4.z : r4.w) << 32) | tag_j;
+            const float d2 = sq_dist<D>(xi, r4);
+            if ((key_j > key_i) && (d2 <= thr))
+              nh_consider(bs, d2, q, key_j);
+          }
+        }
+        if (coop) {
+          first = false;
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            slo[d] = ulo[d];
+            shi[d] = uhi[d];
+          }
+          search = prune_box();
+        }
+      }
+    }
+    while (search) {
       const int t = first ? t0 : tile_id<D>(g, p, ev.tile_base, b);
       const int base = a.tile_offset[t];
       if (a.tile_offset[t + 1] != base) {
@@ -1706,6 +1790,8 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
             c0[d] = cell_coord(xi[d], glo[d], ginv[d], st);
             c_lo[d] = c0[d] - 1;
             c_hi[d] = c0[d] + 1;
+            slo[d] = c_lo[d];
+            shi[d] = c_hi[d];
           } else {
             c_lo[d] = cell_coord(__fsub_rd(xi[d], R), glo[d], ginv[d], st);
             c_hi[d] = cell_coord(__fadd_ru(xi[d], R), glo[d], ginv[d], st);
@@ -1726,44 +1812,33 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
               valid &= cd >= 0 && cd < st;
             }
             lin = lin * st + cd;
-            seen &= abs(cd - c0[d]) <= 1;
+            seen &= cd >= slo[d] && cd <= shi[d];
           }
           if (valid && !seen)
-            visit_cell<D>(a, base + lin, xi, key_i, eff2, bs, cnt);
+            visit_cell<D, STATS>(a, base + lin, xi, key_i, eff2, bs, cnt);
         } while (next_tile<D>(c, c_lo, c_hi));
       }
       if (first) {
-        // Phase 1 visits only the tiles of the box that can hold a point
-        // within reach of the best so far (every point that can still win has
-        // each coordinate within R of the point's, and bins are monotone).
         first = false;
-        const float R = reach(fminf(eff2, bs.hi));
-        bool empty = false;
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          inf[d] = max(inf[d], bin_below(g, __fsub_rd(xi[d], R), d));
-          sup[d] = min(sup[d], bin_above(g, __fadd_ru(xi[d], R), d));
-          b[d] = inf[d];
-          empty |= inf[d] > sup[d];
-        }
-        if (empty)
+        if (!prune_box())
           break;
       } else if (!next_tile<D>(b, inf, sup)) {
         break;
       }
     }
 
-    if (a.stats) {
-      const unsigned am = __activemask();
-      const int members = __reduce_add_sync(am, cnt[2]);
-      const int checked = __reduce_add_sync(am, cnt[0]);
-      const int entered = __reduce_add_sync(am, cnt[1]);
-      if (lane == __ffs(am) - 1) {
+    if (STATS) {  // every lane gets here
+      const int members = __reduce_add_sync(kFullMask, active ? cnt[2] : 0);
+      const int checked = __reduce_add_sync(kFullMask, active ? cnt[0] : 0);
+      const int entered = __reduce_add_sync(kFullMask, active ? cnt[1] : 0);
+      if (lane == 0) {
         atomicAdd(&a.stats[2], (unsigned long long)members);
         atomicAdd(&a.stats[3], (unsigned long long)checked);
         atomicAdd(&a.stats[4], (unsigned long long)entered);
       }
     }
+    if (!active)
+      continue;
     const int gi = a.perm[s];
     const int qb = bs.best >= 0 ? a.nh_q[bs.best] : s;
     const int nh = bs.best >= 0 ? a.perm[qb] : -1;
@@ -1874,17 +1949,17 @@ cudaError_t launch_density_fast(const RunParams& p, const SweepArgs& a, cudaStre
 // Block shapes of the nearest-higher cell search (clue_tuning::nh_shape):
 // 0: 256 threads with 8 blocks per SM in 2-D, 4 in 3-D; 1: 256 threads, 6 per
 // SM; 2: 128 threads with 16 blocks per SM in 2-D, 8 in 3-D.
-template <int D>
+template <int D, bool STATS>
 void launch_nh_cells(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
   switch (p.nh_shape) {
     case 1:
-      k_nearest_higher_cells<D, 256, 6><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
+      k_nearest_higher_cells<D, 256, 6, STATS><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
       break;
     case 2:
-      k_nearest_higher_cells<D, 128, D == 2 ? 16 : 8><<<sweep_grid(a.n, 128, 32), 128, 0, st>>>(p, a);
+      k_nearest_higher_cells<D, 128, D == 2 ? 16 : 8, STATS><<<sweep_grid(a.n, 128, 32), 128, 0, st>>>(p, a);
       break;
     default:
-      k_nearest_higher_cells<D, 256, D == 2 ? 8 : 4><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
+      k_nearest_higher_cells<D, 256, D == 2 ? 8 : 4, STATS><<<sweep_grid(a.n, 256, 16), 256, 0, st>>>(p, a);
       break;
   }
 }
@@ -1905,9 +1980,9 @@ cudaError_t launch_nearest_higher(int D, const RunParams& p, const SweepArgs& a,
   count_launches(1);  // one kernel on every path below
   if (a.nh_cells) {
     if (D == 2)
-      launch_nh_cells<2>(p, a, st);
+      a.stats ? launch_nh_cells<2, true>(p, a, st) : launch_nh_cells<2, false>(p, a, st);
     else
-      launch_nh_cells<3>(p, a, st);
+      a.stats ? launch_nh_cells<3, true>(p, a, st) : launch_nh_cells<3, false>(p, a, st);
     return cudaGetLastError();
   }
   if (sweep_fast_path(p)) {
