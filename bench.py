@@ -308,6 +308,7 @@ def run_ours(args, world, rank, local):
     extras = {}
     if rank == 0 and not args.skip_extras:
         extras = run_extras(args, ev, sizes, local, stream, hbm_peak)
+        extras["configs"] = run_configs(args, local)
         del coords_d, weights_d, pts
         torch.cuda.empty_cache()
         extras["serving"] = run_serving(args, local)
@@ -432,6 +433,45 @@ def run_extras(args, ev, sizes, local, stream, hbm_peak):
         "density_candidate_tests_per_point": sweeps1["density_tests"] / big.n,
         "nearest_higher_members_tested_per_point": sweeps1["nh_members_tested"] / big.n,
     }
+    return out
+
+
+def run_configs(args, local):
+    """The single-event configurations on the GPU (device-resident inputs, median
+    of 20 calls with a sync each) and in the CPU checker on 1 core and on all
+    host cores (median of 3): 16,384-point 2-D, 1,048,576-point 2-D and
+    10,000-hit 3-D layered events."""
+    import torch
+
+    import cluestering_b200 as clue
+    from cluestering_b200 import workloads as W
+    from oracle import oracle as O
+    dev = torch.device("cuda", local)
+    cases = [("single_2d_16384", W.single_2d(), (1.5, 5.0, 1.5), "flat", (0.5,)),
+             ("large_2d_1048576", W.large_2d(), (1.5, 8.0, 2.0), "flat", (0.5,)),
+             ("layered_3d_10000", W.layered_3d(), (3.0, 10.0, 4.0), "gaussian", (1.0, 1.0))]
+    out = {}
+    for name, ev, prm, kern, kp in cases:
+        pts = clue.PointsDevice(torch.from_numpy(ev.coords).to(dev), torch.from_numpy(ev.weights).to(dev),
+                                outputs=("cluster_index",))
+        algo = clue.Clusterer(*prm, device=local)
+        k = clue.FlatKernel(*kp) if kern == "flat" else clue.GaussianKernel(*kp)
+        for _ in range(3):
+            algo.make_clusters(pts, clue.EuclideanMetric(), k)
+        ts = []
+        for _ in range(20):
+            t0 = time.perf_counter()
+            algo.make_clusters(pts, clue.EuclideanMetric(), k)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        row = {"points": ev.n, "gpu_ms": float(np.median(ts))}
+        for cores in (1, os.cpu_count() or 1):
+            cs = []
+            for _ in range(1 if (cores == 1 and ev.n > 100000) else 3):
+                t0 = time.perf_counter()
+                O.make_clusters(ev.coords, ev.weights, *prm, kernel=kern, kernel_params=kp, n_threads=cores)
+                cs.append((time.perf_counter() - t0) * 1e3)
+            row[f"cpu_ms_{cores}_cores" if cores > 1 else "cpu_ms_1_core"] = float(np.median(cs))
+        out[name] = row
     return out
 
 

@@ -1575,26 +1575,6 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, co
 
 // Tests the members of one cell unless the cell is empty, holds no higher
 // key, or its box is out of reach.
-// Bounds on the bin of any coordinate >= c (bin_below) or <= c (bin_above),
-// for a grid without wrapping: get_bin's expression, with the cases where its
-// x86 conversion is not monotone (infinite or NaN quotients, which only a zero
-// tile size or an enormous coordinate give) sent to the widest bound.
-__device__ __forceinline__ int bin_below(const GridDesc& g, float c, int d) {
-  const float u = __fdiv_rn(__fsub_rn(c, g.minv[d]), g.tile[d]);
-  if (!(u < 2147483648.0f))  // NaN or >= 2^31
-    return u == u ? g.k - 1 : 0;
-  return u < 0.0f ? 0 : min((int)u, g.k - 1);
-}
-__device__ __forceinline__ int bin_above(const GridDesc& g, float c, int d) {
-  const float u = __fdiv_rn(__fsub_rn(c, g.minv[d]), g.tile[d]);
-  if (!(u < 2147483648.0f))  // NaN or >= 2^31
-    return g.k - 1;
-  return u < 0.0f ? 0 : min((int)u, g.k - 1);
-}
-
-// Whether the warp runs phase 0 of the cell search as one shared stream.
-constexpr bool kCoopPhase0 = true;
-
 // `cnt` counts cells checked, cells entered and members tested (statistics).
 template <int D, bool STATS>
 __device__ __forceinline__ void visit_cell(const SweepArgs& a, int slot, const float* xi,
@@ -1692,89 +1672,14 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
     // coordinate beyond the int range to bin 0 (x86 conversion), so a huge
     // radius can give a box that misses the point's own tile.
     int c0[D], b[D];
-    int slo[D], shi[D];  // cells of the own tile that phase 0 searched
     bool first = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       b[d] = inf[d];
       c0[d] = 0;
-      slo[d] = 1;
-      shi[d] = 0;
       first &= inf[d] <= own[d] && own[d] <= sup[d];
     }
-    // Phase 1 visits only the tiles of the box that can hold a point within
-    // reach of the best so far (every point that can still win has each
-    // coordinate within R of the point's, and bins are monotone).
-    auto prune_box = [&]() {
-      const float R = reach(fminf(eff2, bs.hi));
-      bool empty = false;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        inf[d] = max(inf[d], bin_below(g, __fsub_rd(xi[d], R), d));
-        sup[d] = min(sup[d], bin_above(g, __fadd_ru(xi[d], R), d));
-        b[d] = inf[d];
-        empty |= inf[d] > sup[d];
-      }
-      return !empty;
-    };
-    bool search = true;
-    if (kCoopPhase0) {
-      // Phase 0 shared by the warp: the lanes whose own tile is lane 0's
-      // (the home tile, in their boxes) stream together the members of the
-      // union of their own cells' neighbourhoods, every record read once for
-      // all of them; each lane tests it with its own key and bounds.
-      const int home = __shfl_sync(kFullMask, t0, 0);
-      const bool coop = first && t0 == home;
-      const int st_h = a.cell_s[home];
-      float glo[D], ginv[D];
-      load_geom<D>(a, home, glo, ginv);
-      int ulo[D], uhi[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        const int cc = cell_coord(xi[d], glo[d], ginv[d], st_h);
-        ulo[d] = max(__reduce_min_sync(kFullMask, coop ? cc : INT_MAX) - 1, 0);
-        uhi[d] = min(__reduce_max_sync(kFullMask, coop ? cc : INT_MIN) + 1, st_h - 1);
-      }
-      if (__any_sync(kFullMask, coop)) {  // warp-uniform
-        const int base_h = a.tile_offset[home];
-        const float thr = coop ? eff2 : -1.0f;  // other lanes take nothing here
-        int rows = uhi[0] - ulo[0] + 1;
-        if (D == 3)
-          rows *= uhi[1] - ulo[1] + 1;
-        for (int r = 0; r < rows; ++r) {
-          int row_cell;
-          if (D == 2) {
-            row_cell = (ulo[0] + r) * st_h;
-          } else {
-            const int n1 = uhi[1] - ulo[1] + 1;
-            row_cell = ((ulo[0] + r / n1) * st_h + ulo[1] + r % n1) * st_h;
-          }
-          const int q0 = a.cell_info[base_h + row_cell + ulo[D - 1]].start;
-          const int q1 = a.cell_info[base_h + row_cell + uhi[D - 1]].end;
-          if (STATS && coop)
-            cnt[2] += q1 - q0;
-#pragma unroll 4
-          for (int q = q0; q < q1; ++q) {
-            const float4 r4 = __ldg(&rec[q]);
-            const uint32_t tag_j = D == 2 ? __float_as_uint(r4.w) : __ldg(&a.rec_tag[q]);
-            const uint64_t key_j = ((uint64_t)__float_as_uint(D == 2 ? r4.z : r4.w) << 32) | tag_j;
-            const float d2 = sq_dist<D>(xi, r4);
-            if ((key_j > key_i) && (d2 <= thr))
-              nh_consider(bs, d2, q, key_j);
-          }
-        }
-        if (coop) {
-          first = false;
-#pragma unroll
-          for (int d = 0; d < D; ++d) {
-            slo[d] = ulo[d];
-            shi[d] = uhi[d];
-          }
-          search = prune_box();
-        }
-      }
-    }
-    while (search) {
+    for (;;) {
       const int t = first ? t0 : tile_id<D>(g, p, ev.tile_base, b);
       const int base = a.tile_offset[t];
       if (a.tile_offset[t + 1] != base) {
@@ -1790,8 +1695,6 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
             c0[d] = cell_coord(xi[d], glo[d], ginv[d], st);
             c_lo[d] = c0[d] - 1;
             c_hi[d] = c0[d] + 1;
-            slo[d] = c_lo[d];
-            shi[d] = c_hi[d];
           } else {
             c_lo[d] = cell_coord(__fsub_rd(xi[d], R), glo[d], ginv[d], st);
             c_hi[d] = cell_coord(__fadd_ru(xi[d], R), glo[d], ginv[d], st);
@@ -1812,19 +1715,16 @@ __global__ void __launch_bounds__(NT, MINB) k_nearest_higher_cells(const RunPara
               valid &= cd >= 0 && cd < st;
             }
             lin = lin * st + cd;
-            seen &= cd >= slo[d] && cd <= shi[d];
+            seen &= abs(cd - c0[d]) <= 1;
           }
           if (valid && !seen)
             visit_cell<D, STATS>(a, base + lin, xi, key_i, eff2, bs, cnt);
         } while (next_tile<D>(c, c_lo, c_hi));
       }
-      if (first) {
+      if (first)
         first = false;
-        if (!prune_box())
-          break;
-      } else if (!next_tile<D>(b, inf, sup)) {
+      else if (!next_tile<D>(b, inf, sup))
         break;
-      }
     }
 
     if (STATS) {  // every lane gets here
