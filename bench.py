@@ -13,8 +13,10 @@ so every step includes the host->device copy of coordinates and weights and the
 device->host copy of the cluster ids. Extra keys report the plain per-event GPU
 form (one make_clusters call per event with a host sync per event, the
 reference's usage pattern), the 1,048,576-point single event and the serving
-loop. With --impl reference the CPU restatement of the reference algorithm
-(oracle/) runs the same workload on all host cores.
+loop. With --impl reference the reference's own make_clusters (oracle/_ref:
+its serial CPU backend compiled from its unmodified headers; the CPU
+restatement in oracle/ where that build is absent) runs a bounded sample of
+the same workload on all host cores, one share of the events per thread.
 
 Under torchrun every rank clusters its own batch (events are independent: no
 collective on the data path); time is the max over ranks and `value` the points
@@ -158,6 +160,48 @@ def cpu_reference(ev, sizes, budget_points: int, threads: int):
             res)
 
 
+def reference_cpu(ev, sizes, budget_points: int, threads: int):
+    """Times the reference's own make_clusters (oracle/_ref: its serial CPU
+    backend, compiled from its unmodified headers) on the first events of the
+    batch, a bounded sample. Like the reference's multi-threaded throughput
+    driver (benchmark/throughput/main.cpp), each of `threads` host threads
+    clusters its own share of the events with its own Clusterer, here through
+    the reference's batched make_clusters. Returns (points/s, sample
+    description, points, events), or None when the build is absent."""
+    from oracle import ref as Rf
+    if not Rf.available():
+        return None
+    total, k = 0, 0
+    while k < len(sizes) and total + int(sizes[k]) <= budget_points:
+        total += int(sizes[k])
+        k += 1
+    k = max(k, 1)
+    offs = np.concatenate([[0], np.cumsum(sizes[:k].astype(np.int64))])
+    total = int(offs[-1])
+    # contiguous shares of about equal points
+    cuts = [0]
+    for t in range(1, threads):
+        cuts.append(int(np.searchsorted(offs, total * t / threads)))
+    cuts.append(k)
+    cuts = sorted(set(cuts))
+    jobs = [(cuts[i], cuts[i + 1]) for i in range(len(cuts) - 1) if cuts[i + 1] > cuts[i]]
+
+    def work(a, b):
+        p0, p1 = int(offs[a]), int(offs[b])
+        Rf.make_clusters_batched(ev.coords[:, p0:p1], ev.weights[p0:p1], sizes[a:b], 1.5, 5.0, 1.5)
+
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=work, args=j) for j in jobs]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    dt = time.perf_counter() - t0
+    return (total / dt, f"first {k} events of the batch ({total} points), {len(jobs)} threads, each "
+                        f"clustering its share of the events with the reference's batched make_clusters",
+            total, k)
+
+
 def parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, ref, n_points, n_events):
     """Clusters the benchmark batch once more with every output requested and
     compares the first `n_events` events (densities as bits, nearest higher,
@@ -188,11 +232,19 @@ def run_reference(args, world, rank):
     ev, sizes = W.batch_2d(n_events=args.events)
     threads = os.cpu_count() or 1
     budget = args.cpu_sample_points
+    from oracle import ref as Rf
+    kind = "reference" if Rf.available() else "port"
+
+    def one(budget_points):
+        if kind == "reference":
+            return reference_cpu(ev, sizes, budget_points, threads)[:3]
+        return cpu_reference(ev, sizes, budget_points, threads)[:3]
+
     for _ in range(args.warmup):
-        cpu_reference(ev, sizes, budget // 4, threads)
+        one(budget // 4)
     vals = []
     for _ in range(args.steps):
-        v, sample, pts, _, _ = cpu_reference(ev, sizes, budget, threads)
+        v, sample, pts = one(budget)
         vals.append(v)
     value = float(np.median(vals))
     line = {
@@ -200,7 +252,7 @@ def run_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": pts / value * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
-        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -303,7 +355,15 @@ def run_ours(args, world, rank, local):
         parity, in_range = parity_sample(algo, coords_d, weights_d, sizes, stream, timed_labels, cpu_res,
                                          cpu_pts, cpu_k)
         del cpu_res
-        ser_val, ser_sample, _, _, _ = cpu_reference(ev, sizes, args.cpu_serial_points, 1)
+        # the reference's own code where it was built, else the restatement
+        ref_all = reference_cpu(ev, sizes, args.cpu_sample_points, threads)
+        cpu_kind = "port"
+        if ref_all is not None:
+            cpu_val, cpu_sample = ref_all[0], ref_all[1]
+            cpu_kind = "reference"
+            ser_val, ser_sample = reference_cpu(ev, sizes, args.cpu_serial_points, 1)[:2]
+        else:
+            ser_val, ser_sample, _, _, _ = cpu_reference(ev, sizes, args.cpu_serial_points, 1)
 
     extras = {}
     if rank == 0 and not args.skip_extras:
@@ -358,7 +418,7 @@ def run_ours(args, world, rank, local):
         "roofline": roof,
         "clocks": clk,
         "cpu_baseline": {"value": cpu_val, "unit": "points/s", "cores": threads,
-                         "kind": "port", "sample": cpu_sample,
+                         "kind": cpu_kind, "sample": cpu_sample,
                          "serial_1_core": {"value": ser_val, "unit": "points/s", "cores": 1,
                                            "sample": ser_sample}},
         "parity_sample": parity,
