@@ -597,11 +597,6 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
     b.grids = piece->grids;
     b.events = piece->events;
     b.chunks = piece->chunks;
-    if (piece->seeds) {
-      b.seeds = piece->seeds;
-      b.seed_event = piece->seed_event;
-      b.status = piece->status;
-    }
   } else {
     const char* err = nullptr;
     if (!build_tables(pts->ndim, sizes, n_events, grid_mode, params->points_per_tile, &own_tables,
@@ -644,8 +639,6 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
     io.piece_base = piece->base;
     io.point_base = piece->point_base;
     io.event_base = piece->event_base;
-    io.labels_after = piece->labels_after;
-    io.labels_done = piece->labels_done;
   }
   io.stats = ws->profiling && !piece ? ws->b.stats : nullptr;
   const RunParams prm = make_run_params(params, pts, ws->tuning);
@@ -815,7 +808,7 @@ std::vector<int32_t> piece_cuts(const uint32_t* sizes, int32_t n_events, int64_t
 clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const clue_points* h,
                             const uint32_t* sizes, cudaStream_t st, const HostTables& whole,
                             const HostTables& all, const std::vector<int32_t>& cuts,
-                            std::vector<Piece>& pieces);
+                            const std::vector<Piece>& pieces);
 
 // The pipelined form of run_host (see kPieceMinPoints). Returns false, having
 // enqueued nothing, when the batch does not split; else the call's status is
@@ -855,20 +848,6 @@ bool run_host_pieces(clue_workspace* ws, const clue_params* params, const clue_p
   if ((int64_t)all.grids.size() > ws->cap.grids || (int64_t)all.events.size() > ws->cap.events ||
       (int64_t)all.chunks.size() > ws->cap.chunks)
     return false;
-  // The odd pieces run on a second workspace (scratch for the largest of
-  // them, no staging: they read and write the first one's staged points), so
-  // that consecutive pieces overlap on the GPU.
-  if (!ws->twin) {
-    clue_status s = clue_workspace_create(&ws->twin, ws->device);
-    if (s != CLUE_OK)
-      return false;
-    ws->twin->tuning = ws->tuning;
-  }
-  ws->twin->tuning = ws->tuning;
-  for (int p = 1; p < P; p += 2)
-    if (ensure_capacity(ws->twin, shapes[p], any_sigma, h->density_uncertainty != nullptr,
-                        h->tags != nullptr, 0) != CLUE_OK)
-      return false;
   std::vector<Piece> pieces(P);
   for (int p = 0; p < P; ++p) {
     Piece& q = pieces[p];
@@ -880,37 +859,26 @@ bool run_host_pieces(clue_workspace* ws, const clue_params* params, const clue_p
     q.grids = ws->b.grids + grid_at[p];
     q.events = ws->b.events + event_at[p];
     q.chunks = ws->b.chunks + chunk_at[p];
-    if (p % 2 == 1) {
-      q.seeds = ws->b.seeds;
-      q.seed_event = ws->b.seed_event;
-      q.status = ws->b.status;
-    }
   }
   *out = pipeline_pieces(ws, params, h, sizes, st, whole, all, cuts, pieces);
   return true;
 }
 
 // Stream order: [tables] on st, then the point uploads of every piece on `up`;
-// piece p clusters once its upload is in (even pieces on st with the first
-// workspace, odd ones on st2 with the second, so consecutive pieces overlap;
-// each piece's label kernel waits for the previous piece's, which moves the
-// shared cluster-id base), and its results go back on `down` once it is
-// clustered, while the next piece clusters.
+// piece p clusters on st once its upload is in, and its results go back on
+// `down` once it is clustered, while the next piece clusters.
 clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const clue_points* h,
                             const uint32_t* sizes, cudaStream_t st, const HostTables& whole,
                             const HostTables& all, const std::vector<int32_t>& cuts,
-                            std::vector<Piece>& pieces) {
+                            const std::vector<Piece>& pieces) {
   const int P = (int)pieces.size();
   cudaError_t e;
   if (!ws->up && (e = cudaStreamCreateWithFlags(&ws->up, cudaStreamNonBlocking)))
     return fail_cuda(e, "upload stream");
   if (!ws->down && (e = cudaStreamCreateWithFlags(&ws->down, cudaStreamNonBlocking)))
     return fail_cuda(e, "download stream");
-  if (!ws->st2 && (e = cudaStreamCreateWithFlags(&ws->st2, cudaStreamNonBlocking)))
-    return fail_cuda(e, "second compute stream");
-  // events: [0] tables up, [1] downloads done, then per piece uploaded,
-  // clustered and labelled
-  const size_t n_ev = 2 + 3 * (size_t)kMaxPieces;
+  // events: [0] tables up, [1] downloads done, then per piece uploaded and clustered
+  const size_t n_ev = 2 + 2 * (size_t)kMaxPieces;
   while (ws->piece_events.size() < n_ev) {
     cudaEvent_t ev;
     if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)))
@@ -918,7 +886,7 @@ clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const
     ws->piece_events.push_back(ev);
   }
   cudaEvent_t* ev = ws->piece_events.data();
-  cudaEvent_t *uploaded = ev + 2, *clustered = ev + 2 + kMaxPieces, *labelled = ev + 2 + 2 * kMaxPieces;
+  cudaEvent_t *uploaded = ev + 2, *clustered = ev + 2 + kMaxPieces;
   clue_status s = stage_tables(ws, all);
   if (s != CLUE_OK)
     return s;
@@ -936,7 +904,6 @@ clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const
   // From here on work is in flight on `up`: every return first waits for it.
   const auto settle = [&](clue_status r) {
     cudaStreamSynchronize(ws->up);
-    cudaStreamSynchronize(ws->st2);
     cudaStreamSynchronize(ws->down);
     return r;
   };
@@ -949,23 +916,16 @@ clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const
   int32_t* base = pieces[0].base;
   if (s == CLUE_OK && (e = launch_fill32(base, 1, 0, st)))
     s = fail_cuda(e, "piece base");
-  // the second stream starts after the base is cleared and the tables are up
-  if (s == CLUE_OK && ((e = cudaEventRecord(ev[1], st)) || (e = cudaStreamWaitEvent(ws->st2, ev[1], 0))))
-    s = fail_cuda(e, "piece ordering");
   int64_t launches = 1;
   for (int p = 0; p < P && s == CLUE_OK; ++p) {
-    clue_workspace* w = p % 2 == 0 ? ws : ws->twin;
-    cudaStream_t sp = p % 2 == 0 ? st : ws->st2;
-    pieces[p].labels_after = p > 0 ? labelled[p - 1] : nullptr;
-    pieces[p].labels_done = labelled[p];
-    if ((e = cudaStreamWaitEvent(sp, uploaded[p], 0))) {
+    if ((e = cudaStreamWaitEvent(st, uploaded[p], 0))) {
       s = fail_cuda(e, "piece ordering");
       break;
     }
-    s = run_device(w, params, &dev[p], sizes + cuts[p], cuts[p + 1] - cuts[p], CLUE_GRID_PER_EVENT,
-                   sp, w == ws ? h->n : 0, &pieces[p]);
-    launches += w->last_launches;
-    if (s == CLUE_OK && (e = cudaEventRecord(clustered[p], sp)))
+    s = run_device(ws, params, &dev[p], sizes + cuts[p], cuts[p + 1] - cuts[p], CLUE_GRID_PER_EVENT,
+                   st, h->n, &pieces[p]);
+    launches += ws->last_launches;
+    if (s == CLUE_OK && (e = cudaEventRecord(clustered[p], st)))
       s = fail_cuda(e, "piece ordering");
   }
   for (int p = 0; p < P && s == CLUE_OK; ++p) {
@@ -1111,15 +1071,13 @@ clue_status clue_workspace_destroy(clue_workspace* ws) {
       cudaEventDestroy(m);
   if (ws->graph_exec)
     cudaGraphExecDestroy(ws->graph_exec);
-  for (cudaStream_t s : {ws->up, ws->down, ws->st2})
+  for (cudaStream_t s : {ws->up, ws->down})
     if (s) {
       cudaStreamSynchronize(s);
       cudaStreamDestroy(s);
     }
   for (cudaEvent_t ev : ws->piece_events)
     cudaEventDestroy(ev);
-  if (ws->twin)
-    clue_workspace_destroy(ws->twin);
   delete ws;
   return CLUE_OK;
 }

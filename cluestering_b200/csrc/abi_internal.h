@@ -52,10 +52,6 @@ struct clue_workspace {
   cudaStream_t up = nullptr, down = nullptr;
   std::vector<cudaEvent_t> piece_events;
   int32_t last_pieces = 0;  // pieces of the last host run (1: not pipelined)
-  // Second workspace and compute stream of pipelined host batches: odd pieces
-  // run there, so a piece's kernels overlap the tail of the one before it.
-  clue_workspace* twin = nullptr;
-  cudaStream_t st2 = nullptr;
 };
 
 namespace clue_impl {
@@ -87,14 +83,6 @@ struct Piece {
   GridDesc* grids = nullptr;
   EventDesc* events = nullptr;
   Chunk* chunks = nullptr;
-  // A piece run on the second workspace of a pipelined batch writes its seeds
-  // and status into the first one's buffers (null: the running workspace's),
-  // and orders its label kernel after the previous piece's (RunIO).
-  int32_t* seeds = nullptr;
-  int32_t* seed_event = nullptr;
-  uint32_t* status = nullptr;
-  cudaEvent_t labels_after = nullptr;
-  cudaEvent_t labels_done = nullptr;
 };
 clue_status run_device(clue_workspace* ws, const clue_params* params, const clue_points* pts,
                        const uint32_t* sizes, int32_t n_events, int32_t grid_mode,

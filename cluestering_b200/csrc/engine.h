@@ -132,12 +132,6 @@ struct RunIO {
   // Sweep statistics: when set, the run zeroes these 8 counters and the sweeps
   // add to them (see SweepArgs::stats).
   unsigned long long* stats = nullptr;
-  // Pieces that run concurrently on two workspaces: the label kernel, which
-  // reads the shared cluster-id base, waits for `labels_after` (the previous
-  // piece moved the base), and `labels_done` is recorded once this piece has
-  // moved it.
-  cudaEvent_t labels_after = nullptr;
-  cudaEvent_t labels_done = nullptr;
 };
 
 // Host tables built for a run.

@@ -1234,8 +1234,6 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     CLUE_LAUNCHED();
   }
   const bool piece = io.piece_base != nullptr;
-  if (io.labels_after)
-    CLUE_CHECK(cudaStreamWaitEvent(st, io.labels_after, 0));
   k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.perm, b.seed_flag, b.seed_rank,
                                              b.point_event, io.cluster_index, b.seeds,
                                              b.seed_event, b.status, io.piece_base,
@@ -1246,8 +1244,6 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     k_advance_piece<<<1, 32, 0, st>>>(io.piece_base, b.counters + 1);
     CLUE_LAUNCHED();
   }
-  if (io.labels_done)
-    CLUE_CHECK(cudaEventRecord(io.labels_done, st));
   CLUE_MARK(6);
 #undef CLUE_MARK
 #undef CLUE_LAUNCHED

@@ -1509,16 +1509,26 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
   // warp, grouped within a round by __match_any_sync; one warp keeps the walk
   // order inside a class, several warps interleave their rounds (any order
   // inside a class is correct: it only decides which lane computes which
-  // point).
+  // point). The class only groups points, so it comes from boxes computed
+  // with a multiplication by the inverse tile size instead of get_bin's
+  // division; the density sweep computes every box exactly.
+  float inv_tile[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    inv_tile[d] = g.tile[d] > 0.0f ? 1.0f / g.tile[d] : 0.0f;
+  auto approx_bin = [&](float x, int d) {
+    const float u = (x - g.minv[d]) * inv_tile[d];
+    return u >= 0.0f ? min((int)fminf(u, (float)g.k), g.k - 1) : 0;  // NaN and below: 0
+  };
   for (int i = tid; i < m; i += NT) {
     const int q = a.nh_q[a.walk[begin + i]];
-    float xq[D];
-    const float zero[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int d = 0; d < D; ++d)
-      xq[d] = a.sx[d * n + q];
     int inf[D], sup[D];
-    search_box<D>(g, p, xq, zero, p.dc, inf, sup);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float x = a.sx[d * n + q];
+      inf[d] = approx_bin(x - p.dc, d);
+      sup[d] = approx_bin(x + p.dc, d);
+    }
     const int c = box_class<D>(g, own, inf, sup);
     a.cls_dens[begin + i] = c;
     atomicAdd(&ccnt[c], 1);

@@ -6,10 +6,11 @@
  * baseline of `bench.py` use as the checker. The product path never links,
  * loads or calls it.
  *
- * Parity status: pinned. The reference cannot be compiled here (every header
- * includes <alpaka/alpaka.hpp>; alpaka, Boost, doctest and fmt are external
- * libraries absent from this machine), so this restatement is checked against
- * the reference's own known-answer tests and its committed truth files
+ * Parity status: pinned. tests/test_reference_build.py checks it bit for bit
+ * against the reference's own make_clusters, compiled from its unmodified
+ * headers on its serial CPU backend (oracle/_ref, built by `make ref` against
+ * the alpaka stand-in in alpaka_shim/), and tests/test_oracle.py against the
+ * reference's own known-answer tests and its committed truth files
  * (tests/golden/).
  *
  * Floating-point semantics are the reference's source-level IEEE-754 single
