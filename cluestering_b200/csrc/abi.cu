@@ -57,6 +57,9 @@ bool grid_shape(int D, int64_t n, int ppt, int32_t* k_out, int64_t* T_out) {
     }
     return p;
   };
+  // the smallest k with k^D >= nt, searched upward from just below the root
+  if (nt > 1)
+    k = std::max<int64_t>(1, (int64_t)std::floor(std::pow((double)nt, 1.0 / D)) - 1);
   while (powk(k) < nt)
     ++k;
   *k_out = (int32_t)k;
@@ -73,6 +76,29 @@ void fill_grid(GridDesc* g, int D, int32_t k, int64_t T) {
     g->stride[d] = s;
     s *= k;
   }
+}
+
+// EventDesc::by_size of events[0, B): largest first, by a counting sort on
+// the size's binary magnitude and next two bits (sizes within 25 % keep index
+// order; the order only balances per-event passes).
+void order_by_size(EventDesc* events, int32_t B) {
+  auto bucket = [](int32_t m) {
+    if (m <= 3)
+      return m;
+    const int lg = 31 - __builtin_clz((uint32_t)m);
+    return 4 * (lg - 1) + ((m >> (lg - 2)) & 3);
+  };
+  constexpr int kBuckets = 4 * 31;
+  int32_t first[kBuckets + 1] = {};
+  for (int e = 0; e < B; ++e)
+    ++first[kBuckets - 1 - bucket(events[e].n)];
+  for (int b = 0, acc = 0; b <= kBuckets; ++b) {
+    const int c = first[b];
+    first[b] = acc;
+    acc += c;
+  }
+  for (int e = 0; e < B; ++e)
+    events[first[kBuckets - 1 - bucket(events[e].n)]++].by_size = e;
 }
 
 bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode, int32_t ppt,
@@ -124,6 +150,10 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
       }
     }
   }
+  int64_t n_chunks = 0;
+  for (int e = 0; e < B; ++e)
+    n_chunks += (t->events[e].n + kChunkPoints - 1) / kChunkPoints;
+  t->chunks.reserve(n_chunks);
   for (int e = 0; e < B; ++e) {
     const EventDesc& ev = t->events[e];
     for (int32_t c = ev.begin; c < ev.begin + ev.n; c += kChunkPoints)
@@ -131,9 +161,10 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
   }
   // Stable binning layout: runs of each event, their warps and count matrices.
   int64_t warps = 0, entries = 0;
-  int32_t max_tiles = 0;
+  int32_t max_tiles = 0, max_points = 0;
   for (int e = 0; e < B; ++e) {
     EventDesc& ev = t->events[e];
+    max_points = std::max(max_points, ev.n);
     const int64_t T = t->grids[ev.grid].T;
     ev.sort_chunks = sort_runs(ev.n, &ev.sort_len);
     ev.sort_first = (int32_t)std::min<int64_t>(warps, INT32_MAX);
@@ -142,10 +173,12 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
     entries += T * ev.sort_chunks;
     max_tiles = (int32_t)std::max<int64_t>(max_tiles, std::min<int64_t>(T, INT32_MAX));
   }
+  order_by_size(t->events.data(), B);
   sh->stable = max_tiles <= kStableMaxTiles && entries <= 4 * N && warps < INT32_MAX;
   sh->sort_warps = (int32_t)std::min<int64_t>(warps, INT32_MAX);
   sh->sort_entries = entries;
   sh->max_event_tiles = max_tiles;
+  sh->max_event_points = max_points;
   sh->D = D;
   sh->n = N;
   sh->n_tiles = tiles;
@@ -590,7 +623,7 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   // the buffers and already on the device.
   HostTables own_tables;
   RunShape own_shape;
-  const HostTables& t = piece ? *piece->tables : own_tables;
+  const HostTables& t = own_tables;  // empty for a piece, whose tables are up already
   const RunShape& sh = piece ? *piece->shape : own_shape;
   DeviceBuffers b = ws->b;
   if (piece) {
@@ -643,6 +676,8 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   io.stats = ws->profiling && !piece ? ws->b.stats : nullptr;
   const RunParams prm = make_run_params(params, pts, ws->tuning);
   reset_launch_count();
+  if (sh.max_event_points <= kLocalLabelPoints)
+    local_labels_ready(sh.max_event_points);  // a device attribute: set before any capture
   if (use_graph && (e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return fail_cuda(e, "stream capture");
   // Everything from here to the end of the capture is stream work.
@@ -690,7 +725,8 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   cudaEventRecord(ws->run_event, st);
   ws->has_run = true;
   ws->last_n = sh.n;
-  ws->last_events = t.events;
+  if (!piece)
+    ws->last_events = t.events;
   ws->last_labels = pts->cluster_index;
   return CLUE_OK;
 }
@@ -780,17 +816,21 @@ namespace {
 constexpr int64_t kPieceMinPoints = int64_t(1) << 22;
 constexpr int kMaxPieces = 4;
 
-// Event boundaries of the pieces: cuts[p] .. cuts[p + 1]. Piece p holds about
-// min(p + 1, 3) shares of the points (1:2:3:3 for four pieces): the first
-// piece is small, so clustering starts after a short upload, and each later
-// piece uploads (about 2.6 times faster than it clusters, on the benchmark
-// batch) while the one before it clusters.
+// Event boundaries of the pieces: cuts[p] .. cuts[p + 1], in shares of the
+// points of 1:2 (two pieces), 1:3:2 (three) and 1:3:6:2 (four). Clustering
+// starts after the first piece's upload and the call ends after the last
+// piece's download, so both are small; the upload of a piece (about 2.9 times
+// faster than its clustering, on the benchmark batch) must still finish
+// while the piece before it clusters, which bounds each share at about 2.9
+// times the one before.
 std::vector<int32_t> piece_cuts(const uint32_t* sizes, int32_t n_events, int64_t n) {
   const int64_t k = std::min<int64_t>({kMaxPieces, n / kPieceMinPoints, n_events});
+  static constexpr int64_t kShares[kMaxPieces + 1][kMaxPieces] = {
+      {0, 0, 0, 0}, {1, 0, 0, 0}, {1, 2, 0, 0}, {1, 3, 2, 0}, {1, 3, 6, 2}};
   std::vector<int64_t> ends;  // cumulative shares
   int64_t shares = 0;
   for (int64_t p = 0; p < k; ++p)
-    ends.push_back(shares += std::min<int64_t>(p + 1, 3));
+    ends.push_back(shares += kShares[k][p]);
   std::vector<int32_t> cuts{0};
   int64_t acc = 0;
   for (int32_t e = 0; e < n_events; ++e) {
@@ -821,29 +861,57 @@ bool run_host_pieces(clue_workspace* ws, const clue_params* params, const clue_p
   if (P < 2)
     return false;
   // Each piece's tables, and all of them end to end: piece p runs on its slice
-  // of the table buffers, so one upload ahead of the points serves every piece.
-  std::vector<HostTables> tabs(P);
+  // of the table buffers, so one upload ahead of the points serves every
+  // piece. With one grid per event a piece's tables are its events' part of
+  // the whole batch's, counted from the piece's first point, tile, event,
+  // chunk and stable-binning run.
+  HostTables all = whole;
   std::vector<RunShape> shapes(P);
   std::vector<int64_t> first(P + 1, 0);
-  HostTables all;
-  std::vector<size_t> grid_at(P), event_at(P), chunk_at(P);
+  std::vector<size_t> chunk_at(P + 1, all.chunks.size());  // chunks are in event order
+  for (size_t k = 0, p = 0; p < (size_t)P; ++p) {
+    while (k < all.chunks.size() && all.chunks[k].event < cuts[p])
+      ++k;
+    chunk_at[p] = k;
+  }
   for (int p = 0; p < P; ++p) {
-    const char* err = nullptr;
-    if (!build_tables(h->ndim, sizes + cuts[p], cuts[p + 1] - cuts[p], CLUE_GRID_PER_EVENT,
-                      params->points_per_tile, &tabs[p], &shapes[p], &err))
-      return false;
-    first[p + 1] = first[p] + shapes[p].n;
+    const int32_t c0 = cuts[p], c1 = cuts[p + 1];
+    const EventDesc e0 = all.events[c0];
+    RunShape& sh = shapes[p];
+    sh.D = h->ndim;
+    sh.n_events = sh.n_grids = c1 - c0;
+    sh.n_chunks = (int32_t)(chunk_at[p + 1] - chunk_at[p]);
+    int64_t warps = 0, entries = 0;
+    for (int32_t e = c0; e < c1; ++e) {
+      EventDesc& ev = all.events[e];
+      const int64_t T = all.grids[e].T;
+      sh.n += ev.n;
+      sh.n_tiles += T;
+      warps += ev.sort_chunks;
+      entries += T * ev.sort_chunks;
+      sh.max_event_tiles = (int32_t)std::max<int64_t>(sh.max_event_tiles, T);
+      sh.max_event_points = std::max(sh.max_event_points, ev.n);
+      ev.begin -= e0.begin;
+      ev.tile_base -= e0.tile_base;
+      ev.grid -= c0;
+      ev.sort_first -= e0.sort_first;
+      ev.sort_base -= e0.sort_base;
+    }
+    order_by_size(all.events.data() + c0, c1 - c0);
+    for (size_t k = chunk_at[p]; k < chunk_at[p + 1]; ++k) {
+      Chunk& c = all.chunks[k];
+      c.event -= c0;
+      c.begin -= e0.begin;
+      c.end -= e0.begin;
+    }
+    sh.stable = sh.max_event_tiles <= kStableMaxTiles && entries <= 4 * sh.n && warps < INT32_MAX;
+    sh.sort_warps = (int32_t)std::min<int64_t>(warps, INT32_MAX);
+    sh.sort_entries = entries;
+    first[p + 1] = first[p] + sh.n;
     // every piece must fit the buffers sized for the whole batch: nothing may
     // be reallocated under the uploads in flight
-    if (!capacity_fits(ws, shapes[p], any_sigma, h->density_uncertainty != nullptr,
-                       h->tags != nullptr, h->n))
+    if (!capacity_fits(ws, sh, any_sigma, h->density_uncertainty != nullptr, h->tags != nullptr, h->n))
       return false;
-    grid_at[p] = all.grids.size();
-    event_at[p] = all.events.size();
-    chunk_at[p] = all.chunks.size();
-    all.grids.insert(all.grids.end(), tabs[p].grids.begin(), tabs[p].grids.end());
-    all.events.insert(all.events.end(), tabs[p].events.begin(), tabs[p].events.end());
-    all.chunks.insert(all.chunks.end(), tabs[p].chunks.begin(), tabs[p].chunks.end());
   }
   if ((int64_t)all.grids.size() > ws->cap.grids || (int64_t)all.events.size() > ws->cap.events ||
       (int64_t)all.chunks.size() > ws->cap.chunks)
@@ -854,10 +922,9 @@ bool run_host_pieces(clue_workspace* ws, const clue_params* params, const clue_p
     q.base = ws->b.counters + 8;
     q.point_base = first[p];
     q.event_base = cuts[p];
-    q.tables = &tabs[p];
     q.shape = &shapes[p];
-    q.grids = ws->b.grids + grid_at[p];
-    q.events = ws->b.events + event_at[p];
+    q.grids = ws->b.grids + cuts[p];
+    q.events = ws->b.events + cuts[p];
     q.chunks = ws->b.chunks + chunk_at[p];
   }
   *out = pipeline_pieces(ws, params, h, sizes, st, whole, all, cuts, pieces);

@@ -78,7 +78,6 @@ struct Piece {
   int32_t* base = nullptr;
   int64_t point_base = 0;
   int32_t event_base = 0;
-  const HostTables* tables = nullptr;
   const RunShape* shape = nullptr;
   GridDesc* grids = nullptr;
   EventDesc* events = nullptr;

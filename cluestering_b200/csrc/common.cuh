@@ -51,6 +51,9 @@ struct EventDesc {
   int32_t sort_chunks;
   int32_t sort_len;
   int32_t sort_base;
+  // The event at position e of the batch's events ordered by size, largest
+  // first (so that per-event passes over a queue start with the longest).
+  int32_t by_size;
 };
 
 // Tiles of one event the stable binning handles: each warp keeps a counter per
@@ -322,6 +325,7 @@ enum : uint32_t {
   kStatusSortOverflow = 1u << 1,
   kStatusLabelTimeout = 1u << 2,
   kStatusCopyTimeout = 1u << 3,
+  kStatusLabelRange = 1u << 4,  // a nearest-higher chain left its event
 };
 
 }  // namespace clue_impl

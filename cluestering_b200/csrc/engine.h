@@ -104,11 +104,20 @@ struct RunShape {
   int32_t sort_warps = 0;
   int64_t sort_entries = 0;
   int32_t max_event_tiles = 0;
+  int32_t max_event_points = 0;  // points of the largest event
 };
 
 // Runs of the stable binning for an event of n points: one per kStableRun
 // points, at least one. Returns the run count; *len = points per run.
 int32_t sort_runs(int64_t n, int32_t* len);
+
+// Largest event whose labels launch_run walks in shared memory (one grid per
+// event); local_labels_ready(points) grants that kernel the shared memory of
+// an event of `points` points on the current device (outside stream capture,
+// once per device). False when the device refuses: the run then labels in
+// global memory.
+constexpr int32_t kLocalLabelPoints = 1 << 16;
+bool local_labels_ready(int32_t points);
 
 // Pointers of one run's inputs and outputs (device memory).
 struct RunIO {

@@ -10,7 +10,9 @@
 //   density sweep : rho per point, summed in the reference's exact order
 //   NH sweep      : nearest higher, the reference's comparisons and tie-breaks
 //   seeds/labels  : exclusive scan of the seed flags (seed k = k-th seed in
-//                   index order gets cluster id k), roots by pointer jumping.
+//                   index order gets cluster id k), roots by pointer jumping
+//                   (per event in shared memory when every event has its own
+//                   grid and at most 65,536 points; else over the whole run).
 #include <atomic>
 #include <cfloat>
 #include <cuda/atomic>
@@ -934,6 +936,101 @@ __global__ void k_labels(int64_t n, int32_t* parent, const int32_t* perm, const 
   }
 }
 
+// Labels of a run whose events each occupy their own range of the layout (one
+// grid per event: event e's points are layout positions [begin, begin + n),
+// and every nearest-higher chain stays inside its event) and hold at most
+// kLocalLabelPoints points. A block takes one event at a time from a queue
+// (largest first, so the longest ones do not run as a tail),
+// copies the event's part of `parent` into shared memory as 16-bit event-local
+// positions, and shortens every chain there by pointer-jumping rounds (every
+// write stores an ancestor, so in-place rounds stay valid). The chains
+// never touch global memory again: the global form above re-reads `parent`
+// from L2 at every step and needs whole-array jumping rounds before it. The
+// outputs are those of k_labels.
+constexpr int kLocalLabelThreads = 1024;
+constexpr int kLabelBatch = 4;
+constexpr int kLabelRounds = 20;
+
+__global__ void __launch_bounds__(kLocalLabelThreads, 1)
+    k_labels_local(const EventDesc* events, int32_t n_events, int32_t* queue, const int32_t* parent,
+                   const int32_t* perm, const int32_t* seed_flag, const int32_t* seed_rank,
+                   const int32_t* point_event, int32_t* cluster_index, int32_t* seeds,
+                   int32_t* seed_event, uint32_t* status, const int32_t* piece_base,
+                   int32_t point_base, int32_t event_base, int32_t* nh) {
+  extern __shared__ uint16_t up[];  // event-local parent of each point of the event
+  __shared__ int s_event;
+  const int32_t base = piece_base ? *piece_base : 0;
+  for (;;) {
+    if (threadIdx.x == 0)
+      s_event = atomicAdd(queue, 1);
+    __syncthreads();
+    const int e = s_event;
+    if (e >= n_events)
+      break;
+    const EventDesc ev = events[events[e].by_size];
+    const int b = ev.begin, m = ev.n;
+    bool outside = false;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      const int q = parent[b + i] - b;
+      outside |= (unsigned)q >= (unsigned)m;
+      up[i] = (uint16_t)((unsigned)q < (unsigned)m ? q : i);
+    }
+    if (outside)  // a chain leaving its event: never, for one grid per event
+      atomicOr(status, kStatusLabelRange);
+    __syncthreads();
+    // chains: pointer-jumping rounds over the whole event (a round at least
+    // halves every path, so 17 rounds reach the root of any chain of at most
+    // 65,536 points; more means a cycle, which is reported) until every point
+    // sits on its root. Rounds run over all points at once, so their shared-
+    // memory loads overlap instead of following one chain at a time.
+    for (int round = 0;; ++round) {
+      int moved = 0;
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int q = up[i];
+        const int qq = up[q];
+        if (qq != q) {
+          up[i] = (uint16_t)qq;
+          moved = 1;
+        }
+      }
+      if (!__syncthreads_or(moved))
+        break;
+      if (round == kLabelRounds) {
+        if (threadIdx.x == 0)
+          atomicOr(status, kStatusLabelTimeout);
+        break;
+      }
+    }
+    // outputs, kLabelBatch points per thread at a time so that their global
+    // loads are in flight together
+    for (int i0 = threadIdx.x; i0 < m; i0 += kLabelBatch * blockDim.x) {
+      int gi[kLabelBatch], gr[kLabelBatch];
+#pragma unroll
+      for (int u = 0; u < kLabelBatch; ++u) {
+        const int i = i0 + u * blockDim.x;
+        gi[u] = gr[u] = -1;
+        if (i < m) {
+          gi[u] = perm[b + i];
+          gr[u] = perm[b + up[i]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kLabelBatch; ++u) {
+        if (gi[u] < 0)
+          continue;
+        cluster_index[gi[u]] = seed_flag[gr[u]] ? seed_rank[gr[u]] + base : -1;
+        if (seed_flag[gi[u]]) {
+          seeds[seed_rank[gi[u]] + base] = gi[u] + point_base;
+          seed_event[seed_rank[gi[u]] + base] = point_event[gi[u]] + event_base;
+        }
+        if (nh && nh[gi[u]] >= 0)
+          nh[gi[u]] += point_base;
+      }
+    }
+    __syncthreads();  // up[] and s_event are rewritten for the next event
+  }
+}
+
 // Moves a piece's base past its seeds, for the next piece of the batch.
 __global__ void k_advance_piece(int32_t* piece_base, const int32_t* n_seeds) {
   if (threadIdx.x == 0)
@@ -1023,6 +1120,29 @@ int sm_count() {
     cache[dev].store(v, std::memory_order_relaxed);
   }
   return v;
+}
+
+// Lets k_labels_local take the shared memory of an event of `points` points
+// on the current device (above the default 48 KB it needs the opt-in, set
+// once per device for the largest event size). False when the device refuses.
+bool local_labels_ready(int32_t points) {
+  const size_t smem = ((size_t)std::max(points, 1) * sizeof(uint16_t) + 15) & ~(size_t)15;
+  if (smem <= (48u << 10))
+    return true;
+  constexpr int kDevices = 64;
+  static std::atomic<int> granted[kDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices)
+    return false;
+  const int need = (int)(((size_t)kLocalLabelPoints * sizeof(uint16_t)));
+  if (granted[dev].load(std::memory_order_relaxed) < need) {
+    if (cudaFuncSetAttribute(k_labels_local, cudaFuncAttributeMaxDynamicSharedMemorySize, need) != cudaSuccess) {
+      cudaGetLastError();  // the refusal is not left pending for the next launch
+      return false;
+    }
+    granted[dev].store(need, std::memory_order_relaxed);
+  }
+  return true;
 }
 
 int scan_blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile); }
@@ -1223,23 +1343,38 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
 
   // seeds and labels
   CLUE_CHECK(scan(b.seed_flag, b.seed_rank, n, b.counters + 1, b, st));
-  // Large runs first shorten every chain with whole-array jumping rounds, so
-  // the per-point walks below take a few steps; small runs walk directly.
-  const int jump_rounds = prm.jump_rounds >= 0                ? prm.jump_rounds
-                          : n >= (int64_t)1 << 22 ? 3
-                          : n >= (int64_t)1 << 18 ? 2
-                                                  : 0;
-  for (int r = 0; r < jump_rounds; ++r) {
-    k_jump<<<grid_for(n), kThreads, 0, st>>>(n, b.parent);
+  const bool piece = io.piece_base != nullptr;
+  int32_t* nh_shift = piece && io.point_base ? io.nh : nullptr;
+  // One grid per event keeps every event in its own range of the layout: the
+  // chains are walked per event in shared memory.
+  const bool local_labels = sh.n_grids == sh.n_events && sh.max_event_points <= kLocalLabelPoints &&
+                            local_labels_ready(sh.max_event_points);
+  if (local_labels) {
+    const size_t smem = ((size_t)std::max(sh.max_event_points, 1) * sizeof(uint16_t) + 15) & ~(size_t)15;
+    const int blocks = std::max(1, std::min(sh.n_events, sm_count() * (smem <= (96u << 10) ? 2 : 1)));
+    CLUE_CHECK(fill32(b.counters + 6, 1, 0, st));
+    k_labels_local<<<blocks, kLocalLabelThreads, smem, st>>>(
+        b.events, sh.n_events, b.counters + 6, b.parent, b.perm, b.seed_flag, b.seed_rank,
+        b.point_event, io.cluster_index, b.seeds, b.seed_event, b.status, io.piece_base,
+        (int32_t)io.point_base, io.event_base, nh_shift);
+    CLUE_LAUNCHED();
+  } else {
+    // Large runs first shorten every chain with whole-array jumping rounds, so
+    // the per-point walks below take a few steps; small runs walk directly.
+    const int jump_rounds = prm.jump_rounds >= 0                ? prm.jump_rounds
+                            : n >= (int64_t)1 << 22 ? 3
+                            : n >= (int64_t)1 << 18 ? 2
+                                                    : 0;
+    for (int r = 0; r < jump_rounds; ++r) {
+      k_jump<<<grid_for(n), kThreads, 0, st>>>(n, b.parent);
+      CLUE_LAUNCHED();
+    }
+    k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.perm, b.seed_flag, b.seed_rank,
+                                               b.point_event, io.cluster_index, b.seeds,
+                                               b.seed_event, b.status, io.piece_base,
+                                               (int32_t)io.point_base, io.event_base, nh_shift);
     CLUE_LAUNCHED();
   }
-  const bool piece = io.piece_base != nullptr;
-  k_labels<<<grid_for(n), kThreads, 0, st>>>(n, b.parent, b.perm, b.seed_flag, b.seed_rank,
-                                             b.point_event, io.cluster_index, b.seeds,
-                                             b.seed_event, b.status, io.piece_base,
-                                             (int32_t)io.point_base, io.event_base,
-                                             piece && io.point_base ? io.nh : nullptr);
-  CLUE_LAUNCHED();
   if (piece) {
     k_advance_piece<<<1, 32, 0, st>>>(io.piece_base, b.counters + 1);
     CLUE_LAUNCHED();

@@ -81,6 +81,7 @@ extern "C" clue_status clue_make_clusters_device_noalloc(const clue_params* para
   sh.sort_warps = ev.sort_chunks;
   sh.sort_entries = T * (int64_t)ev.sort_chunks;
   sh.max_event_tiles = (int32_t)T;
+  sh.max_event_points = (int32_t)n;
   sh.stable = T <= kStableMaxTiles && sh.sort_entries <= 4 * n;
 
   bool any_sigma = false;

@@ -918,13 +918,20 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
     // Any order is exact here. Every record in range adds its v_j, the
     // point's own record included; the own term is corrected once at the end.
     if (cnt == kChunk && __all_sync(kFullMask, acc == 0xffffffffu)) {
+      // two running sums (exact, so their split and final sum change
+      // nothing): measured 3 % faster than one
+      float rho_b = 0.0f;
 #pragma unroll 8
-      for (int j = 0; j < kChunk; ++j) {
-        float v;
+      for (int j = 0; j < kChunk; j += 2) {
+        float v, v1;
         const float d2 = packed_d2<D>(xi_xy, xi[2], chunk[j], v);
+        const float d2b = packed_d2<D>(xi_xy, xi[2], chunk[j + 1], v1);
         if (d2 <= p.dc2)
           rho = __fadd_rn(rho, v);
+        if (d2b <= p.dc2)
+          rho_b = __fadd_rn(rho_b, v1);
       }
+      rho = __fadd_rn(rho, rho_b);
     } else {
       for (int j = 0; j < cnt; ++j) {
         float v;
@@ -1509,26 +1516,16 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
   // warp, grouped within a round by __match_any_sync; one warp keeps the walk
   // order inside a class, several warps interleave their rounds (any order
   // inside a class is correct: it only decides which lane computes which
-  // point). The class only groups points, so it comes from boxes computed
-  // with a multiplication by the inverse tile size instead of get_bin's
-  // division; the density sweep computes every box exactly.
-  float inv_tile[D];
-#pragma unroll
-  for (int d = 0; d < D; ++d)
-    inv_tile[d] = g.tile[d] > 0.0f ? 1.0f / g.tile[d] : 0.0f;
-  auto approx_bin = [&](float x, int d) {
-    const float u = (x - g.minv[d]) * inv_tile[d];
-    return u >= 0.0f ? min((int)fminf(u, (float)g.k), g.k - 1) : 0;  // NaN and below: 0
-  };
+  // point).
   for (int i = tid; i < m; i += NT) {
     const int q = a.nh_q[a.walk[begin + i]];
-    int inf[D], sup[D];
+    float xq[D];
+    const float zero[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      const float x = a.sx[d * n + q];
-      inf[d] = approx_bin(x - p.dc, d);
-      sup[d] = approx_bin(x + p.dc, d);
-    }
+    for (int d = 0; d < D; ++d)
+      xq[d] = a.sx[d * n + q];
+    int inf[D], sup[D];
+    search_box<D>(g, p, xq, zero, p.dc, inf, sup);
     const int c = box_class<D>(g, own, inf, sup);
     a.cls_dens[begin + i] = c;
     atomicAdd(&ccnt[c], 1);
@@ -1556,10 +1553,14 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
 // than kLargeTilePoints points, which the tile sort listed, one block each, so
 // a dense tile of thousands of points does not hold up the launch on one warp;
 // they come first so that the heaviest tiles do not run as a tail. The other
-// blocks give one warp to each smaller tile.
+// blocks give one warp to each smaller tile. The kernel waits on dependent
+// loads, so it trades registers for resident blocks: in 2-D 6 blocks per SM
+// (40 registers, 8 bytes spilled) took 2.2 ms of the 46.5 M-point batch
+// against 2.7 ms at the compiler's 64 registers (4 blocks); the 3-D form keeps
+// 4, where 5 spills more and measured slower.
 constexpr int kWarpCellSlots = kLargeTilePoints;  // s^D <= m <= 256 (at least 1 point per cell)
 template <int D>
-__global__ void __launch_bounds__(kCellWarps * 32) k_cells(const RunParams p, const SweepArgs a,
+__global__ void __launch_bounds__(kCellWarps * 32, D == 2 ? 6 : 4) k_cells(const RunParams p, const SweepArgs a,
                                                           int large_blocks) {
   constexpr int E = box_classes<D>();
   static_assert(kWarpCellSlots * kCellWarps <= kCellSlots, "warp counters fit the block's");
