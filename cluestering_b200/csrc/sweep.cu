@@ -1516,16 +1516,25 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
   // warp, grouped within a round by __match_any_sync; one warp keeps the walk
   // order inside a class, several warps interleave their rounds (any order
   // inside a class is correct: it only decides which lane computes which
-  // point).
+  // point). The class only groups points, so it comes from boxes computed
+  // with a multiplication by the inverse tile size instead of get_bin's
+  // division (a point near a tile boundary may land in a neighbouring class);
+  // the density sweep computes every box exactly.
+  float inv_tile[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    inv_tile[d] = g.tile[d] > 0.0f ? 1.0f / g.tile[d] : 0.0f;
   for (int i = tid; i < m; i += NT) {
     const int q = a.nh_q[a.walk[begin + i]];
-    float xq[D];
-    const float zero[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int d = 0; d < D; ++d)
-      xq[d] = a.sx[d * n + q];
     int inf[D], sup[D];
-    search_box<D>(g, p, xq, zero, p.dc, inf, sup);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float x = a.sx[d * n + q];
+      const float u0 = (x - p.dc - g.minv[d]) * inv_tile[d];
+      const float u1 = (x + p.dc - g.minv[d]) * inv_tile[d];
+      inf[d] = u0 >= 0.0f ? min((int)fminf(u0, (float)g.k), g.k - 1) : 0;  // NaN and below: 0
+      sup[d] = u1 >= 0.0f ? min((int)fminf(u1, (float)g.k), g.k - 1) : 0;
+    }
     const int c = box_class<D>(g, own, inf, sup);
     a.cls_dens[begin + i] = c;
     atomicAdd(&ccnt[c], 1);
