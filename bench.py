@@ -3,7 +3,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 A step is one batched make_clusters over the batch_2d workload: 4,096 2-D
-events of log-uniform size in [256, 65,536] (~48 M points), unit weights,
+events of log-uniform size in [256, 65,536] (46.5 M points), unit weights,
 dc = 1.5, rhoc = 5, dm = 1.5, flat kernel, one tile grid per event. Inputs are
 larger than L2 (126 MB), so no flush is needed between steps.
 
@@ -50,17 +50,17 @@ CONFIG = {
 # index and writes nh (4D + 12); the whole pipeline moves 20D + 64.
 BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4 * D + 12,
                    "pipeline": lambda D: 20 * D + 64}
-# DRAM bytes (read + write) per point of each sweep, from ncu captures of the
-# 1,024-event batch (profiles/sweeps_batch_2d_1024ev.md: 922.5 MB for density;
-# profiles/nearest_higher_and_cells_batch_2d_1024ev.md: 703.2 MB for nearest
-# higher; 10,621,973 points); a launch's traffic grows with the points it processes.
-DRAM_BYTES_PER_POINT = {"density": 86.9, "nearest_higher": 66.2}
+# DRAM bytes (read + write) per point of each sweep, from one ncu capture
+# (--set full) of the 1,024-event batch (10,621,973 points): 922.4 MB for the
+# density sweep, 739.2 MB for the nearest-higher search; a launch's traffic
+# grows with the points it processes.
+DRAM_BYTES_PER_POINT = {"density": 86.8, "nearest_higher": 69.6}
 # Warp instructions per point of each sweep (smsp__inst_executed.sum / points),
-# from the same captures: 2.76 G for density, 1.72 G for nearest higher over
-# 10,621,973 points. The sweeps are bound by instruction issue: the issue
-# roofline is SMs x 4 schedulers x one warp instruction per cycle at the SM
-# clock sampled during the timed steps.
-INST_PER_POINT = {"density": 259.8, "nearest_higher": 161.9}
+# from the same capture: 2.783 G for density, 1.609 G for nearest higher. The
+# sweeps are bound by instruction issue: the issue roofline is SMs x 4
+# schedulers x one warp instruction per cycle at the SM clock sampled during
+# the timed steps.
+INST_PER_POINT = {"density": 262.0, "nearest_higher": 151.4}
 
 
 def measured_peaks():
