@@ -832,12 +832,16 @@ std::vector<int32_t> piece_cuts(const uint32_t* sizes, int32_t n_events, int64_t
   for (int64_t p = 0; p < k; ++p)
     ends.push_back(shares += kShares[k][p]);
   std::vector<int32_t> cuts{0};
-  int64_t acc = 0;
+  int64_t acc = 0, at_cut = 0;
   for (int32_t e = 0; e < n_events; ++e) {
     acc += sizes[e];
     const size_t p = cuts.size() - 1;  // the piece this event ends up in
-    if ((int64_t)p + 1 < k && e + 1 < n_events && acc * shares >= ends[p] * n)
+    // every piece holds points: events of size 0 never make a piece alone
+    if ((int64_t)p + 1 < k && e + 1 < n_events && acc * shares >= ends[p] * n && acc > at_cut &&
+        acc < n) {
       cuts.push_back(e + 1);
+      at_cut = acc;
+    }
   }
   cuts.push_back(n_events);
   return cuts;

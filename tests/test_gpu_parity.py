@@ -297,6 +297,37 @@ def test_sample_associations_full_csr_mixed_batch():
         assert np.array_equal(offsets, expected_sample_offsets(o, len(sizes)))
 
 
+def with_empty_events(sizes, where):
+    """`sizes` with a batch item of size 0 inserted before each position in
+    `where` (len(sizes) appends one at the end)."""
+    out = [int(s) for s in sizes]
+    for pos in sorted(where, reverse=True):
+        out.insert(pos, 0)
+    return np.array(out, np.uint32)
+
+
+@pytest.mark.parametrize("mode", [clue.GRID_PER_EVENT, clue.GRID_SHARED])
+@pytest.mark.parametrize("binning", [0, 1])
+def test_batch_with_empty_events(mode, binning):
+    # Batch items of size 0 at the start, inside and at the end: the reference
+    # scans the sizes as given (core/detail/Clusterer.hpp:293-300), so such an
+    # item holds no points and no clusters, and the associator's key count
+    # stops at the last event with a cluster (MakeAssociator.hpp:32-43).
+    ev, sizes = W.batch_2d(24, 256, 8192, seed=31)
+    sizes = with_empty_events(sizes, [0, 0, 5, 12, 12, 12, len(sizes), len(sizes)])
+    w = np.random.default_rng(32).exponential(1.0, ev.n).astype(np.float32)
+    for weights in (ev.weights, w):  # exact-sum and ordered density sums
+        c = clue.Clusterer(1.5, 5.0, 1.5)
+        c.set_tuning(tile_binning=binning)
+        for path in ("host", "device"):
+            g, o = check(ev.coords, weights, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=mode, path=path,
+                         clusterer=c)
+            offsets, n_keys = g["clusterer"].getSampleAssociations()
+            ea = np.asarray(o.event_associations)
+            assert n_keys == (int(ea[-1]) + 1 if len(ea) else 0) < len(sizes)
+            assert np.array_equal(offsets, expected_sample_offsets(o, len(sizes)))
+
+
 @pytest.mark.parametrize("name", ["data_4096", "data_32768"])
 def test_reference_datasets(name):
     c, w = fixture(name)
@@ -456,6 +487,14 @@ def test_pipelined_host_batch_equals_the_device_batch():
     # their whole-batch numbering
     ev, sizes = W.batch_2d(640, 4096, 32768, seed=61)
     assert ev.n >= 1 << 23
+    assert _pipelined_against_device(ev, sizes, (1.5, 5.0, 1.5), clue.FlatKernel(0.5)) >= 2
+
+
+def test_pipelined_host_batch_with_empty_events():
+    # items of size 0 among and after the events: every piece still holds
+    # points (a piece of empty items alone would launch empty grids)
+    ev, sizes = W.batch_2d(640, 4096, 32768, seed=61)
+    sizes = with_empty_events(sizes, [0, 1, 64, 64, 200, 320, 321, 500] + [len(sizes)] * 3)
     assert _pipelined_against_device(ev, sizes, (1.5, 5.0, 1.5), clue.FlatKernel(0.5)) >= 2
 
 
