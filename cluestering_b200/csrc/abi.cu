@@ -817,16 +817,17 @@ constexpr int64_t kPieceMinPoints = int64_t(1) << 22;
 constexpr int kMaxPieces = 4;
 
 // Event boundaries of the pieces: cuts[p] .. cuts[p + 1], in shares of the
-// points of 1:2 (two pieces), 1:3:2 (three) and 1:3:6:2 (four). Clustering
+// points of 1:2 (two pieces), 1:3:2 (three) and 1:3:8:1 (four). Clustering
 // starts after the first piece's upload and the call ends after the last
 // piece's download, so both are small; the upload of a piece (about 2.9 times
 // faster than its clustering, on the benchmark batch) must still finish
 // while the piece before it clusters, which bounds each share at about 2.9
-// times the one before.
+// times the one before. Downloads move 4 bytes per point against 12 up, so
+// the last piece's download hides a share up to about 8.7 times its own.
 std::vector<int32_t> piece_cuts(const uint32_t* sizes, int32_t n_events, int64_t n) {
   const int64_t k = std::min<int64_t>({kMaxPieces, n / kPieceMinPoints, n_events});
   static constexpr int64_t kShares[kMaxPieces + 1][kMaxPieces] = {
-      {0, 0, 0, 0}, {1, 0, 0, 0}, {1, 2, 0, 0}, {1, 3, 2, 0}, {1, 3, 6, 2}};
+      {0, 0, 0, 0}, {1, 0, 0, 0}, {1, 2, 0, 0}, {1, 3, 2, 0}, {1, 3, 8, 1}};
   std::vector<int64_t> ends;  // cumulative shares
   int64_t shares = 0;
   for (int64_t p = 0; p < k; ++p)
