@@ -188,6 +188,27 @@ bool build_tables(int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode
   return true;
 }
 
+// The tables of a batch shape in ws->tables: rebuilt only when the dimension,
+// grid mode, points per tile or event sizes differ from the last build's
+// (a batch of the same shape has the same tables). False, with *err set, when
+// build_tables rejects the shape.
+bool shape_tables(clue_workspace* ws, int32_t D, const uint32_t* sizes, int32_t B, int32_t grid_mode,
+                  int32_t ppt, const char** err) {
+  clue_workspace::TableCache& c = ws->tables;
+  if (c.valid && c.D == D && c.grid_mode == grid_mode && c.ppt == ppt &&
+      c.sizes.size() == (size_t)std::max(B, 0) && std::equal(sizes, sizes + B, c.sizes.begin()))
+    return true;
+  c.valid = c.split = false;
+  if (!build_tables(D, sizes, B, grid_mode, ppt, &c.tables, &c.shape, err))
+    return false;
+  c.sizes.assign(sizes, sizes + B);
+  c.D = D;
+  c.grid_mode = grid_mode;
+  c.ppt = ppt;
+  c.valid = true;
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Workspace memory
 // ---------------------------------------------------------------------------
@@ -621,20 +642,19 @@ clue_status run_device(clue_workspace* ws, const clue_params* params, const clue
   ws->graph_replays_last = false;
   // A piece of a pipelined batch comes with its tables built, checked against
   // the buffers and already on the device.
-  HostTables own_tables;
-  RunShape own_shape;
-  const HostTables& t = own_tables;  // empty for a piece, whose tables are up already
-  const RunShape& sh = piece ? *piece->shape : own_shape;
+  const HostTables& t = ws->tables.tables;  // unused by a piece, whose tables are up already
+  if (!piece) {
+    const char* err = nullptr;
+    if (!shape_tables(ws, pts->ndim, sizes, n_events, grid_mode, params->points_per_tile, &err))
+      return fail(CLUE_ERR_INVALID_ARGUMENT, err);
+  }
+  const RunShape& sh = piece ? *piece->shape : ws->tables.shape;
   DeviceBuffers b = ws->b;
   if (piece) {
     b.grids = piece->grids;
     b.events = piece->events;
     b.chunks = piece->chunks;
   } else {
-    const char* err = nullptr;
-    if (!build_tables(pts->ndim, sizes, n_events, grid_mode, params->points_per_tile, &own_tables,
-                      &own_shape, &err))
-      return fail(CLUE_ERR_INVALID_ARGUMENT, err);
     if (sh.n != pts->n)
       return fail(CLUE_ERR_INVALID_ARGUMENT, "the event sizes do not add up to the number of points");
     bool any_sigma = false;
@@ -861,78 +881,90 @@ clue_status pipeline_pieces(clue_workspace* ws, const clue_params* params, const
 bool run_host_pieces(clue_workspace* ws, const clue_params* params, const clue_points* h,
                      const uint32_t* sizes, int32_t n_events, cudaStream_t st,
                      const HostTables& whole, bool any_sigma, clue_status* out) {
-  const std::vector<int32_t> cuts = piece_cuts(sizes, n_events, h->n);
-  const int P = (int)cuts.size() - 1;
+  // The split depends on the tables alone: it is made once per table build
+  // (ws->tables, whose tables `whole` are) and reused by calls of the same shape.
+  clue_workspace::TableCache& c = ws->tables;
+  if (!c.split) {
+    c.cuts = piece_cuts(sizes, n_events, h->n);
+    const int P = (int)c.cuts.size() - 1;
+    if (P >= 2) {
+      // Each piece's tables, and all of them end to end: piece p runs on its
+      // slice of the table buffers, so one upload ahead of the points serves
+      // every piece. With one grid per event a piece's tables are its events'
+      // part of the whole batch's, counted from the piece's first point, tile,
+      // event, chunk and stable-binning run.
+      HostTables& all = c.all;
+      all = whole;
+      c.shapes.assign(P, RunShape{});
+      c.first.assign(P + 1, 0);
+      c.chunk_at.assign(P + 1, all.chunks.size());  // chunks are in event order
+      for (size_t k = 0, p = 0; p < (size_t)P; ++p) {
+        while (k < all.chunks.size() && all.chunks[k].event < c.cuts[p])
+          ++k;
+        c.chunk_at[p] = k;
+      }
+      for (int p = 0; p < P; ++p) {
+        const int32_t c0 = c.cuts[p], c1 = c.cuts[p + 1];
+        const EventDesc e0 = all.events[c0];
+        RunShape& sh = c.shapes[p];
+        sh.D = h->ndim;
+        sh.n_events = sh.n_grids = c1 - c0;
+        sh.n_chunks = (int32_t)(c.chunk_at[p + 1] - c.chunk_at[p]);
+        int64_t warps = 0, entries = 0;
+        for (int32_t e = c0; e < c1; ++e) {
+          EventDesc& ev = all.events[e];
+          const int64_t T = all.grids[e].T;
+          sh.n += ev.n;
+          sh.n_tiles += T;
+          warps += ev.sort_chunks;
+          entries += T * ev.sort_chunks;
+          sh.max_event_tiles = (int32_t)std::max<int64_t>(sh.max_event_tiles, T);
+          sh.max_event_points = std::max(sh.max_event_points, ev.n);
+          ev.begin -= e0.begin;
+          ev.tile_base -= e0.tile_base;
+          ev.grid -= c0;
+          ev.sort_first -= e0.sort_first;
+          ev.sort_base -= e0.sort_base;
+        }
+        order_by_size(all.events.data() + c0, c1 - c0);
+        for (size_t k = c.chunk_at[p]; k < c.chunk_at[p + 1]; ++k) {
+          Chunk& ch = all.chunks[k];
+          ch.event -= c0;
+          ch.begin -= e0.begin;
+          ch.end -= e0.begin;
+        }
+        sh.stable = sh.max_event_tiles <= kStableMaxTiles && entries <= 4 * sh.n && warps < INT32_MAX;
+        sh.sort_warps = (int32_t)std::min<int64_t>(warps, INT32_MAX);
+        sh.sort_entries = entries;
+        c.first[p + 1] = c.first[p] + sh.n;
+      }
+    }
+    c.split = true;
+  }
+  const int P = (int)c.cuts.size() - 1;
   if (P < 2)
     return false;
-  // Each piece's tables, and all of them end to end: piece p runs on its slice
-  // of the table buffers, so one upload ahead of the points serves every
-  // piece. With one grid per event a piece's tables are its events' part of
-  // the whole batch's, counted from the piece's first point, tile, event,
-  // chunk and stable-binning run.
-  HostTables all = whole;
-  std::vector<RunShape> shapes(P);
-  std::vector<int64_t> first(P + 1, 0);
-  std::vector<size_t> chunk_at(P + 1, all.chunks.size());  // chunks are in event order
-  for (size_t k = 0, p = 0; p < (size_t)P; ++p) {
-    while (k < all.chunks.size() && all.chunks[k].event < cuts[p])
-      ++k;
-    chunk_at[p] = k;
-  }
-  for (int p = 0; p < P; ++p) {
-    const int32_t c0 = cuts[p], c1 = cuts[p + 1];
-    const EventDesc e0 = all.events[c0];
-    RunShape& sh = shapes[p];
-    sh.D = h->ndim;
-    sh.n_events = sh.n_grids = c1 - c0;
-    sh.n_chunks = (int32_t)(chunk_at[p + 1] - chunk_at[p]);
-    int64_t warps = 0, entries = 0;
-    for (int32_t e = c0; e < c1; ++e) {
-      EventDesc& ev = all.events[e];
-      const int64_t T = all.grids[e].T;
-      sh.n += ev.n;
-      sh.n_tiles += T;
-      warps += ev.sort_chunks;
-      entries += T * ev.sort_chunks;
-      sh.max_event_tiles = (int32_t)std::max<int64_t>(sh.max_event_tiles, T);
-      sh.max_event_points = std::max(sh.max_event_points, ev.n);
-      ev.begin -= e0.begin;
-      ev.tile_base -= e0.tile_base;
-      ev.grid -= c0;
-      ev.sort_first -= e0.sort_first;
-      ev.sort_base -= e0.sort_base;
-    }
-    order_by_size(all.events.data() + c0, c1 - c0);
-    for (size_t k = chunk_at[p]; k < chunk_at[p + 1]; ++k) {
-      Chunk& c = all.chunks[k];
-      c.event -= c0;
-      c.begin -= e0.begin;
-      c.end -= e0.begin;
-    }
-    sh.stable = sh.max_event_tiles <= kStableMaxTiles && entries <= 4 * sh.n && warps < INT32_MAX;
-    sh.sort_warps = (int32_t)std::min<int64_t>(warps, INT32_MAX);
-    sh.sort_entries = entries;
-    first[p + 1] = first[p] + sh.n;
-    // every piece must fit the buffers sized for the whole batch: nothing may
-    // be reallocated under the uploads in flight
-    if (!capacity_fits(ws, sh, any_sigma, h->density_uncertainty != nullptr, h->tags != nullptr, h->n))
+  // every piece must fit the buffers sized for the whole batch: nothing may
+  // be reallocated under the uploads in flight
+  for (int p = 0; p < P; ++p)
+    if (!capacity_fits(ws, c.shapes[p], any_sigma, h->density_uncertainty != nullptr, h->tags != nullptr,
+                       h->n))
       return false;
-  }
-  if ((int64_t)all.grids.size() > ws->cap.grids || (int64_t)all.events.size() > ws->cap.events ||
-      (int64_t)all.chunks.size() > ws->cap.chunks)
+  if ((int64_t)c.all.grids.size() > ws->cap.grids || (int64_t)c.all.events.size() > ws->cap.events ||
+      (int64_t)c.all.chunks.size() > ws->cap.chunks)
     return false;
   std::vector<Piece> pieces(P);
   for (int p = 0; p < P; ++p) {
     Piece& q = pieces[p];
     q.base = ws->b.counters + 8;
-    q.point_base = first[p];
-    q.event_base = cuts[p];
-    q.shape = &shapes[p];
-    q.grids = ws->b.grids + cuts[p];
-    q.events = ws->b.events + cuts[p];
-    q.chunks = ws->b.chunks + chunk_at[p];
+    q.point_base = c.first[p];
+    q.event_base = c.cuts[p];
+    q.shape = &c.shapes[p];
+    q.grids = ws->b.grids + c.cuts[p];
+    q.events = ws->b.events + c.cuts[p];
+    q.chunks = ws->b.chunks + c.chunk_at[p];
   }
-  *out = pipeline_pieces(ws, params, h, sizes, st, whole, all, cuts, pieces);
+  *out = pipeline_pieces(ws, params, h, sizes, st, whole, c.all, c.cuts, pieces);
   return true;
 }
 
@@ -1035,11 +1067,11 @@ clue_status run_host(clue_workspace* ws, const clue_params* params, const clue_p
   if ((s = check_points(h, true, params->metric_kind)) != CLUE_OK)
     return s;
   // Make sure the staging buffers exist before copying into them.
-  HostTables t;
-  RunShape sh;
   const char* err = nullptr;
-  if (!build_tables(h->ndim, sizes, n_events, grid_mode, params->points_per_tile, &t, &sh, &err))
+  if (!shape_tables(ws, h->ndim, sizes, n_events, grid_mode, params->points_per_tile, &err))
     return fail(CLUE_ERR_INVALID_ARGUMENT, err);
+  const HostTables& t = ws->tables.tables;
+  const RunShape& sh = ws->tables.shape;
   if (sh.n != h->n)
     return fail(CLUE_ERR_INVALID_ARGUMENT, "the event sizes do not add up to the number of points");
   bool any_sigma = false;

@@ -52,6 +52,22 @@ struct clue_workspace {
   cudaStream_t up = nullptr, down = nullptr;
   std::vector<cudaEvent_t> piece_events;
   int32_t last_pieces = 0;  // pieces of the last host run (1: not pipelined)
+  // Tables of the last batch shape (dimension, grid mode, points per tile,
+  // event sizes), reused by a call with the same shape, and the pipelined
+  // split of those tables once a host call has made it.
+  struct TableCache {
+    bool valid = false;
+    int32_t D = 0, grid_mode = 0, ppt = 0;
+    std::vector<uint32_t> sizes;
+    clue_impl::HostTables tables;
+    clue_impl::RunShape shape;
+    bool split = false;             // the fields below belong to these tables
+    std::vector<int32_t> cuts;      // event boundaries of the pieces
+    clue_impl::HostTables all;      // the tables counted from each piece's start
+    std::vector<clue_impl::RunShape> shapes;
+    std::vector<int64_t> first;     // first point of each piece
+    std::vector<size_t> chunk_at;   // first chunk of each piece
+  } tables;
 };
 
 namespace clue_impl {

@@ -498,6 +498,33 @@ def test_pipelined_host_batch_with_empty_events():
     assert _pipelined_against_device(ev, sizes, (1.5, 5.0, 1.5), clue.FlatKernel(0.5)) >= 2
 
 
+def test_reused_tables_follow_the_batch_shape():
+    # One clusterer keeps the tables (and the pipelined split) of the last batch
+    # shape; a call with other event sizes over the same points must rebuild
+    # them, and a return to the first shape must give the first results again.
+    ev, sizes = W.batch_2d(640, 4096, 32768, seed=65)
+    merged = np.concatenate([[sizes[0] + sizes[1]], sizes[2:]]).astype(np.uint32)
+    n = ev.n
+
+    def run(c, sz):
+        h = clue.PointsHost(ev.coords, ev.weights)
+        h.is_seed = np.zeros(n, np.int32)
+        h.rho = np.zeros(n, np.float32)
+        h.nearest_higher = np.zeros(n, np.int32)
+        c.make_clusters(h, batch_item_sizes=sz, grid_mode=clue.GRID_PER_EVENT)
+        return dict(ci=h.cluster_index.copy(), rho=h.rho.view(np.int32).copy(), nh=h.nearest_higher.copy(),
+                    seed=h.is_seed.copy(), assoc=c.getSampleAssociations()[0], pieces=c.host_pieces())
+
+    fresh = {k: run(clue.Clusterer(1.5, 5.0, 1.5), sz) for k, sz in (("a", sizes), ("b", merged))}
+    reused = clue.Clusterer(1.5, 5.0, 1.5)
+    for k in ("a", "b", "a", "a", "b"):
+        got = run(reused, sizes if k == "a" else merged)
+        for f in ("ci", "rho", "nh", "seed", "assoc"):
+            assert np.array_equal(got[f], fresh[k][f]), (k, f)
+        assert got["pieces"] == fresh[k]["pieces"] >= 2
+    assert not np.array_equal(fresh["a"]["assoc"][:3], fresh["b"]["assoc"][:3])
+
+
 def test_pipelined_host_batch_equals_the_device_batch_3d_gaussian():
     evs = [W.layered_3d(int(m), seed=70 + i) for i, m in
            enumerate(W.log_uniform_sizes(160, 16384, 131072, seed=71))]
