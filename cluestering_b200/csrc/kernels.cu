@@ -857,8 +857,44 @@ __global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int
                                                      const int32_t* point_event, float* sx,
                                                      float* sw, float* ssig, float* sunc,
                                                      uint32_t* stag, int32_t* sevt) {
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-       s += (int64_t)gridDim.x * blockDim.x) {
+  // Two-dimensional runs with no per-point options (the common case) take
+  // four points per thread a grid-stride apart, every gather issued before
+  // any store, so more of this memory pass is in flight.
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  if (D == 2 && !has_sigma && !unc && !tags) {
+    constexpr int U = 4;
+    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s0 < n; s0 += U * stride) {
+      int i[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        i[u] = s0 + u * stride < n ? perm[s0 + u * stride] : 0;
+      float vx[U], vy[U], vw[U];
+      int ve[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        vx[u] = vy[u] = vw[u] = 0.0f;
+        ve[u] = 0;
+        if (s0 + u * stride < n) {
+          vx[u] = x.p[0][i[u]];
+          vy[u] = x.p[1][i[u]];
+          vw[u] = w[i[u]];
+          ve[u] = point_event[i[u]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t s = s0 + u * stride;
+        if (s >= n)
+          break;
+        sx[s] = vx[u];
+        sx[n + s] = vy[u];
+        sw[s] = vw[u];
+        sevt[s] = ve[u];
+      }
+    }
+    return;
+  }
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
     const int i = perm[s];
     for (int d = 0; d < D; ++d)
       sx[d * n + s] = x.p[d][i];
