@@ -856,7 +856,18 @@ __global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int
                                                      const uint32_t* tags,
                                                      const int32_t* point_event, float* sx,
                                                      float* sw, float* ssig, float* sunc,
-                                                     uint32_t* stag, int32_t* sevt) {
+                                                     uint32_t* stag, int32_t* sevt, float4* rec,
+                                                     int32_t flat, float flat_p0, int32_t* queue) {
+  // The density records of the fast sweeps (rec, D = 2: {x, y, v, w}; D = 3:
+  // {x, y, z, v}, v = fl(flat * w) for the flat kernel, ConvolutionalKernel.hpp:
+  // 24-27, else w) come from the same loads, and the sweeps' work queues start
+  // empty (queue[0], queue[1]).
+  if (queue && blockIdx.x == 0 && threadIdx.x < 2)
+    queue[threadIdx.x] = 0;
+  auto record = [&](int64_t s, float x0, float x1, float x2, float wt) {
+    const float v = flat ? __fmul_rn(flat_p0, wt) : wt;
+    rec[s] = D == 2 ? make_float4(x0, x1, v, wt) : make_float4(x0, x1, x2, v);
+  };
   // Two-dimensional runs with no per-point options (the common case) take
   // four points per thread a grid-stride apart, every gather issued before
   // any store, so more of this memory pass is in flight.
@@ -890,6 +901,8 @@ __global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int
         sx[n + s] = vy[u];
         sw[s] = vw[u];
         sevt[s] = ve[u];
+        if (rec)
+          record(s, vx[u], vy[u], 0.0f, vw[u]);
       }
     }
     return;
@@ -900,6 +913,8 @@ __global__ void __launch_bounds__(kThreads) k_gather(int D, int64_t n, const int
       sx[d * n + s] = x.p[d][i];
     sw[s] = w[i];
     sevt[s] = point_event[i];
+    if (rec && (D == 2 || D == 3))
+      record(s, x.p[0][i], x.p[1][i], D == 3 ? x.p[2][i] : 0.0f, w[i]);
     if (has_sigma)
       for (int d = 0; d < D; ++d)
         ssig[d * n + s] = ((has_sigma >> d) & 1) ? sig.p[d][i] : 0.0f;
@@ -1321,7 +1336,10 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
   k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
                                              io.unc, io.tags, b.point_event, b.sorted_coords,
                                              b.sorted_weight, b.sorted_sigma, b.sorted_unc,
-                                             b.sorted_tag, b.sorted_event);
+                                             b.sorted_tag, b.sorted_event,
+                                             sweep_fast_path(prm) ? b.rec_dens : nullptr,
+                                             prm.kernel_kind == CLUE_KERNEL_FLAT, prm.kernel_p0,
+                                             b.counters + 4);
   CLUE_LAUNCHED();
 
   // the two sweeps

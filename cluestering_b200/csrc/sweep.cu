@@ -363,33 +363,6 @@ __device__ __forceinline__ float sq_dist(const float* xi, const float4& r) {
   return __fadd_rn(sx, __fadd_rn(sy, __fmul_rn(dz, dz)));
 }
 
-// Density records, in sorted order and (with the cell layout) in cell-layout
-// order.
-template <int D>
-__global__ void __launch_bounds__(kThreads) k_pack_density(const RunParams p, const SweepArgs a) {
-  if (blockIdx.x == 0 && threadIdx.x < 2)
-    a.queue[threadIdx.x] = 0;  // the sweeps that follow start with no item taken
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
-       s += (int64_t)gridDim.x * blockDim.x) {
-    const float w = a.sw[s];
-    // flat: contribution of a neighbour is fl(flat * w_j) (ConvolutionalKernel.hpp:24-27)
-    const float v = p.kernel_kind == CLUE_KERNEL_FLAT ? __fmul_rn(p.kernel_p0, w) : w;
-    float4 r;
-    r.x = a.sx[s];
-    r.y = a.sx[a.n + s];
-    if (D == 2) {
-      r.z = v;
-      r.w = w;
-    } else {
-      r.z = a.sx[2 * a.n + s];
-      r.w = v;
-    }
-    a.rec_dens[s] = r;
-    if (a.rec_cell)
-      a.rec_cell[a.nh_pos[s]] = r;
-  }
-}
-
 // Row iteration shared by both fast sweeps: calls body(q) for every candidate
 // of the search box in the reference's order.
 template <int D, typename Body>
@@ -1456,6 +1429,7 @@ __device__ void tile_cells(const RunParams& p, const SweepArgs& a, int64_t t, in
     const int pos = begin + atomicAdd(&cnt[a.cell_slot[q] - begin], 1);
     a.nh_pos[q] = pos;
     a.nh_q[pos] = q;
+    a.rec_cell[pos] = a.rec_dens[q];  // the density record in cell-layout order
   }
   group_sync<NT>();
   // Member boxes. A point with a NaN coordinate is never within reach and
@@ -1850,8 +1824,7 @@ void launch_density_kind(const RunParams& p, const SweepArgs& a, cudaStream_t st
 
 template <int D>
 cudaError_t launch_density_fast(const RunParams& p, const SweepArgs& a, cudaStream_t st) {
-  k_pack_density<D><<<grid_for(a.n), kThreads, 0, st>>>(p, a);
-  count_launches(2);  // this and the density kernel below
+  count_launches(1);  // the density kernel below; k_gather wrote its records
   switch (p.kernel_kind) {
     case CLUE_KERNEL_FLAT:
       launch_density_kind<D, CLUE_KERNEL_FLAT>(p, a, st);

@@ -28,7 +28,7 @@ struct SweepArgs {
   int32_t* cls_dens;  // scratch: box class per sorted position
   int32_t* cls_nh;
   // Work queues of the fast-path sweeps: [0] density, [1] nearest higher;
-  // each counts the 32-point work items taken so far (k_pack_density resets
+  // each counts the 32-point work items taken so far (k_gather resets
   // both), so warps that finish early take the next item.
   int32_t* queue;
   // Tiles of more than 256 points (listed by the tile sort) and their count:
