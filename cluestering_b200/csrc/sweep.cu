@@ -704,7 +704,7 @@ template <int D>
 __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const EventDesc& ev,
                               const GridDesc& g, const float* xi, int s, float wi, const int* inf,
                               const int* sup, bool ordered, const int* uinf, const int* usup,
-                              float4 (*ring)[kChunk], int* off, int* qa, int* seg, int4* tinfo,
+                              float4 (*ring)[kChunk], int* off, int* qa, int* seg,
                               float& rho, int& tested) {
   const int lane = threadIdx.x & 31;
   int nu[D];
@@ -758,20 +758,42 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
       rows_t = (chi[0] - clo[0] + 1) * (D == 3 ? chi[1] - clo[1] + 1 : 1);
     }
   }
-  int incl = rows_t;
+  // tiles of the union box inside this lane's box, as a mask over union tiles
+  uint32_t tmask = 0;
+  if (ordered) {
+    if (D == 2) {
+      const uint32_t row = (uint32_t)((1ull << (sup[1] - inf[1] + 1)) - 1) << (inf[1] - uinf[1]);
+      for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
+        tmask |= row << ((b0 - uinf[0]) * nu[1]);
+    } else {
+      const uint32_t row = (uint32_t)((1ull << (sup[2] - inf[2] + 1)) - 1) << (inf[2] - uinf[2]);
+      for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
+        for (int b1 = inf[1]; b1 <= sup[1]; ++b1)
+          tmask |= row << (((b0 - uinf[0]) * nu[1] + (b1 - uinf[1])) * nu[2]);
+    }
+  }
+  const uint32_t all_tiles = (uint32_t)((1ull << n_union) - 1);
+  // The tiles in every lane's box stream first (any order sums exactly here):
+  // every lane takes all their records, with no per-lane test.
+  const uint32_t common = __reduce_and_sync(kFullMask, tmask) & all_tiles;
+  const bool is_common = (common >> lane) & 1u;
+  int incl_c = is_common ? rows_t : 0, incl_o = is_common ? 0 : rows_t;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(kFullMask, incl, o);
-    if (lane >= o)
-      incl += y;
+    const int yc = __shfl_up_sync(kFullMask, incl_c, o);
+    const int yo = __shfl_up_sync(kFullMask, incl_o, o);
+    if (lane >= o) {
+      incl_c += yc;
+      incl_o += yo;
+    }
   }
-  const int K = __shfl_sync(kFullMask, incl, 31);
+  const int K_common = __shfl_sync(kFullMask, incl_c, 31);
+  const int K = K_common + __shfl_sync(kFullMask, incl_o, 31);
   if (K > kMaxSegs)
     return false;
-  const int first = incl - rows_t;
+  const int first = is_common ? incl_c - rows_t : K_common + incl_o - rows_t;
   const int n1c = D == 3 ? chi[1] - clo[1] + 1 : 1;
   if (lane < n_union) {
-    tinfo[lane] = make_int4(first, clo[0], D == 3 ? clo[1] : 0, n1c);
     for (int r = 0; r < rows_t; ++r) {
       const int c0 = clo[0] + r / n1c;
       const int row_cell = D == 2 ? c0 * ts : (c0 * ts + clo[1] + r % n1c) * ts;
@@ -802,51 +824,20 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
   if (lane == 0)
     off[K] = total;
   __syncwarp();
-  // tiles of the union box inside this lane's box, as a mask over union tiles
-  uint32_t tmask = 0;
-  if (ordered) {
-    if (D == 2) {
-      const uint32_t row = (uint32_t)((1ull << (sup[1] - inf[1] + 1)) - 1) << (inf[1] - uinf[1]);
-      for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
-        tmask |= row << ((b0 - uinf[0]) * nu[1]);
-    } else {
-      const uint32_t row = (uint32_t)((1ull << (sup[2] - inf[2] + 1)) - 1) << (inf[2] - uinf[2]);
-      for (int b0 = inf[0]; b0 <= sup[0]; ++b0)
-        for (int b1 = inf[1]; b1 <= sup[1]; ++b1)
-          tmask |= row << (((b0 - uinf[0]) * nu[1] + (b1 - uinf[1])) * nu[2]);
-    }
-  }
-  const uint32_t all_tiles = (uint32_t)((1ull << n_union) - 1);
-  // stream position of the point itself: its cell's row segment in its tile
-  // (a point with a non-finite coordinate has nothing in range, itself
-  // included, and needs none)
-  int p_self = -1;
-  {
-    int own[D], t_own = 0;
-    bool in = ordered;
+  const int p_common = off[K_common];  // stream positions [0, p_common): common tiles
+  // Whether the point's own record is among its candidates: a finite point
+  // inside its own box (its cell is within reach of the warp's points and its
+  // tile is in the union); a point with a non-finite coordinate has nothing in
+  // range, itself included.
+  bool self_in = ordered;
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      own[d] = get_bin(g, p, xi[d], d);
-      in &= inf[d] <= own[d] && own[d] <= sup[d] && isfinite(xi[d]);
-      t_own = t_own * nu[d] + (own[d] - uinf[d]);
-    }
-    if (in) {
-      int tile = ev.tile_base;
-#pragma unroll
-      for (int d = 0; d < D; ++d)
-        tile += own[d] * g.stride[d];
-      const int4 ti = tinfo[t_own];
-      const int sq = a.cell_s[tile];
-      const int c = a.cell_slot[s] - a.tile_offset[tile];
-      const int c0 = D == 2 ? c / sq : c / (sq * sq);
-      const int c1 = D == 2 ? 0 : (c / sq) % sq;
-      const int k = ti.x + (c0 - ti.y) * ti.w + (D == 3 ? c1 - ti.z : 0);
-      if (k >= 0 && k < K)  // always, for a finite point inside its box
-        p_self = off[k] + (a.nh_pos[s] - qa[k]);
-    }
+  for (int d = 0; d < D; ++d) {
+    const int own = get_bin(g, p, xi[d], d);
+    self_in &= inf[d] <= own && own <= sup[d] && isfinite(xi[d]);
   }
-  // cursor over this lane's accepted segments: [ilo, ihi) in stream positions
-  int kc = 0, ilo = INT_MAX, ihi = INT_MAX;
+  // cursor over this lane's accepted segments past the common ones: [ilo,
+  // ihi) in stream positions
+  int kc = K_common, ilo = INT_MAX, ihi = INT_MAX;
   auto next_accepted = [&]() {
     while (kc < K && !((tmask >> seg[kc]) & 1u))
       ++kc;
@@ -876,9 +867,9 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
     const int base = c * kChunk;
     const int cnt = min(kChunk, total - base);
     unsigned acc = 0xffffffffu;
-    if (!take_all) {
+    if (!take_all && base + cnt > p_common) {
       const int cend = base + cnt;
-      acc = 0;
+      acc = base < p_common ? range_bits(0, p_common - base) : 0u;
       while (ilo < cend) {
         const int lo = max(ilo, base), hi = min(ihi, cend);
         if (lo < hi)
@@ -920,7 +911,7 @@ __device__ bool density_exact(const RunParams& p, const SweepArgs& a, const Even
   // The own record (d2 = 0, in range) added v_i = fl(flat * w_i) where the
   // reference adds w_i: (rho - v_i) + w_i, both steps exact (multiples of u,
   // between 0 and the event bound).
-  if (p_self >= 0)
+  if (self_in)
     rho = __fadd_rn(__fsub_rn(rho, __fmul_rn(p.kernel_p0, wi)), wi);
   return true;
 }
@@ -938,7 +929,6 @@ __global__ void __launch_bounds__(NT, MINB) k_density_fast(const RunParams p, co
   __shared__ int s_off[NT / 32][kMaxStream + 1];
   __shared__ int s_qa[NT / 32][kMaxStream];
   __shared__ int s_seg[NT / 32][kMaxSegs];
-  __shared__ int4 s_tinfo[NT / 32][kMaxUnionTiles];
   const int64_t n = a.n;
   const float4* __restrict__ rec = a.rec_dens;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1012,7 +1002,7 @@ __global__ void __launch_bounds__(NT, MINB) k_density_fast(const RunParams p, co
     int tested = 0;     // candidate records this lane tests
     if (exact)
       done = density_exact<D>(p, a, ev, g, xi, s, wi, inf, sup, ordered, uinf, usup, ring, off, qa,
-                              s_seg[warp], s_tinfo[warp], rho, tested);
+                              s_seg[warp], rho, tested);
     bool streamed = false;  // warp-uniform: the ordered stream handles the warp
     if (!done && one_grid && rows64 >= 1 && rows64 <= kMaxRows) {
       const int rows = (int)rows64;
