@@ -137,14 +137,37 @@ __global__ void __launch_bounds__(kThreads) k_bin(RunParams p, CoordPtrs x, cons
   const bool bounds = event_exact && p.kernel_kind == CLUE_KERNEL_FLAT;  // block-uniform
   int lsb = INT_MAX, bad = 0;
   uint32_t vb = 0, wb = 0;
+  // 2-D: the coordinates of four rounds are loaded ahead of their binning
+  constexpr int U = 4;
+  float px[U], py[U];
   for (int base = c.begin; base < c.end; base += blockDim.x) {
+    const int k = ((base - c.begin) / (int)blockDim.x) % U;
+    if (p.D == 2 && k == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int iu = base + u * (int)blockDim.x + (int)threadIdx.x;
+        px[u] = iu < c.end ? x.p[0][iu] : 0.0f;
+        py[u] = iu < c.end ? x.p[1][iu] : 0.0f;
+      }
+    }
     const int i = base + threadIdx.x;
     const bool valid = i < c.end;
     int t = -1;
     if (valid) {
       int b = ev.tile_base;
-      for (int d = 0; d < p.D; ++d)
-        b += sg.stride[d] * get_bin(sg, p, x.p[d][i], d);
+      if (p.D == 2) {
+        float vx = px[0], vy = py[0];
+#pragma unroll
+        for (int u = 1; u < U; ++u)
+          if (k == u) {
+            vx = px[u];
+            vy = py[u];
+          }
+        b += sg.stride[0] * get_bin(sg, p, vx, 0) + sg.stride[1] * get_bin(sg, p, vy, 1);
+      } else {
+        for (int d = 0; d < p.D; ++d)
+          b += sg.stride[d] * get_bin(sg, p, x.p[d][i], d);
+      }
       t = b;
       tile_of[i] = t;
       point_event[i] = c.event;
