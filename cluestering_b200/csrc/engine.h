@@ -64,7 +64,8 @@ struct DeviceBuffers {
   // scan state
   unsigned long long* scan_desc = nullptr;
   int32_t* counters = nullptr;     // [0] scan ticket, [1] n_seeds, [2] oversize count, [3] large count,
-                                   // [4..5] sweep work queues, [8] cluster-id base of a pipelined piece
+                                   // [4..5] sweep work queues, [6] label queue, [7] some event not
+                                   // order-free (tile sorts), [8] cluster-id base of a pipelined piece
   int32_t* large_tiles = nullptr;  // tiles too large for the per-warp sort
   int32_t* oversize = nullptr;     // tiles needing a chunk merge
   uint32_t* status = nullptr;

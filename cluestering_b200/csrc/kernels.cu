@@ -691,6 +691,21 @@ __device__ __forceinline__ bool order_free(const int32_t* event_exact, const int
   return event_sums_exact(event_exact, e, events[e].n);
 }
 
+// Sets *some_ordered when any event of the run is not order-free (its sums
+// are not exact in any order, event_sums_exact): one block, which clears the
+// word first.
+__global__ void k_events_order_free(const int32_t* event_exact, const EventDesc* events, int n_events,
+                                    int32_t* some_ordered) {
+  if (threadIdx.x == 0)
+    *some_ordered = 0;
+  __syncthreads();
+  int ordered = 0;
+  for (int e = threadIdx.x; e < n_events; e += blockDim.x)
+    ordered |= !event_sums_exact(event_exact, e, events[e].n);
+  if (__syncthreads_or(ordered) && threadIdx.x == 0)
+    *some_ordered = 1;
+}
+
 // Orders the ids of every tile ascending. One warp per tile: tiles of up to
 // kWarpSortCap ids are rank-sorted by the warp with no block barrier; larger
 // tiles are listed for k_tile_sort_large (and for k_cells, which gives each a
@@ -701,10 +716,13 @@ __global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offs
                                                         int32_t* perm, int32_t* large,
                                                         int32_t* large_count, const int32_t* event_exact,
                                                         const int32_t* point_event,
-                                                        const EventDesc* events) {
+                                                        const EventDesc* events,
+                                                        const int32_t* some_ordered) {
   __shared__ __align__(16) int s_ids[kThreads / 32][kWarpSortCap];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* ids = s_ids[warp];
+  // every event order-free: no tile is sorted, only the large ones listed
+  const bool all_free = event_exact && *some_ordered == 0;
   const int64_t stride = (int64_t)gridDim.x * (kThreads / 32);
   for (int64_t t = (int64_t)blockIdx.x * (kThreads / 32) + warp; t < n_tiles; t += stride) {
     const int begin = tile_offset[t], end = tile_offset[t + 1];
@@ -716,7 +734,7 @@ __global__ void __launch_bounds__(kThreads) k_tile_sort(const int32_t* tile_offs
         large[atomicAdd(large_count, 1)] = (int32_t)t;
       continue;
     }
-    if (order_free(event_exact, point_event, events, perm, begin))
+    if (all_free || order_free(event_exact, point_event, events, perm, begin))
       continue;
     int unsorted = 0;
     for (int i = lane; i < m; i += 32) {
@@ -804,8 +822,11 @@ __global__ void __launch_bounds__(kThreads) k_tile_sort_large(const int32_t* til
                                                               int32_t* oversize_count,
                                                               const int32_t* event_exact,
                                                               const int32_t* point_event,
-                                                              const EventDesc* events) {
+                                                              const EventDesc* events,
+                                                              const int32_t* some_ordered) {
   __shared__ int s[kSortCap];
+  if (event_exact && *some_ordered == 0)
+    return;  // every event order-free
   const int count = *large_count;
   for (int e = blockIdx.x; e < count; e += gridDim.x) {
     const int t = large[e];
@@ -1155,21 +1176,27 @@ cudaError_t scan(const int32_t* in, int32_t* out, int64_t n, int32_t* total,
 // With `event_exact`, segments are tiles and those of exact-sum events keep
 // their order (order_free).
 cudaError_t sort_segments(const int32_t* offsets, int64_t n_segments, int32_t* ids,
-                          const DeviceBuffers& b, cudaStream_t st, const int32_t* event_exact = nullptr) {
+                          const DeviceBuffers& b, cudaStream_t st, const int32_t* event_exact = nullptr,
+                          int n_events = 0) {
   int32_t* oversize_count = b.counters + 2;
   int32_t* large_count = b.counters + 3;
+  int32_t* some_ordered = b.counters + 7;
   cudaError_t e = fill32(oversize_count, 2, 0, st);  // and large_count, the next counter
   if (e != cudaSuccess)
     return e;
+  if (event_exact) {
+    k_events_order_free<<<1, 1024, 0, st>>>(event_exact, b.events, n_events, some_ordered);
+    count_launches(1);
+  }
   const int64_t warps_per_block = kThreads / 32;
   const int blocks =
       (int)std::max<int64_t>(1, std::min<int64_t>((n_segments + warps_per_block - 1) / warps_per_block,
                                                   (int64_t)sm_count() * 16));
   k_tile_sort<<<blocks, kThreads, 0, st>>>(offsets, n_segments, ids, b.large_tiles, large_count,
-                                           event_exact, b.point_event, b.events);
+                                           event_exact, b.point_event, b.events, some_ordered);
   k_tile_sort_large<<<sm_count() * 8, kThreads, 0, st>>>(offsets, b.large_tiles, large_count, ids,
                                                   b.oversize, oversize_count, event_exact,
-                                                  b.point_event, b.events);
+                                                  b.point_event, b.events, some_ordered);
   k_tile_merge<<<sm_count(), kThreads, 0, st>>>(offsets, b.oversize, oversize_count, ids, b.merge_tmp);
   k_tile_merge_copy<<<sm_count(), kThreads, 0, st>>>(offsets, b.oversize, oversize_count, b.merge_tmp,
                                               ids);
@@ -1353,7 +1380,8 @@ cudaError_t launch_run(const RunShape& sh, const RunParams& prm, const RunIO& io
     // Exact-sum events need no ascending order within their tiles when nothing
     // else on this run reads it (flat kernel, cell path: no user tags).
     const bool order_free_tiles = sweep_cells_path(prm) && prm.kernel_kind == CLUE_KERNEL_FLAT;
-    CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st, order_free_tiles ? exact : nullptr));
+    CLUE_CHECK(sort_segments(b.tile_offset, sh.n_tiles, b.perm, b, st, order_free_tiles ? exact : nullptr,
+                             sh.n_events));
   }
   CLUE_MARK(2);
   k_gather<<<grid_for(n), kThreads, 0, st>>>(D, n, b.perm, x, io.weight, sig, prm.has_sigma,
