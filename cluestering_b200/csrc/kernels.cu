@@ -78,11 +78,68 @@ __global__ void k_grid_init(int32_t* grid_minmax, int n_grids, int32_t* event_ex
     event_exact[i] = (i & 3) == 0 ? INT_MAX : 0;
 }
 
+// 2-D and 3-D: one pass over the chunk loads every coordinate of a point, and
+// one shared-memory round reduces all 2 D extremes of the block.
+template <int DD>
+__device__ __forceinline__ void minmax_fixed(CoordPtrs x, const Chunk& c, int g, int32_t* grid_minmax) {
+  __shared__ float red[2 * DD][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float mn[DD], mx[DD];
+#pragma unroll
+  for (int d = 0; d < DD; ++d) {
+    mn[d] = FLT_MAX;
+    mx[d] = -FLT_MAX;
+  }
+  for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
+#pragma unroll
+    for (int d = 0; d < DD; ++d) {
+      const float v = x.p[d][i];
+      if (v == v) {  // NaN never becomes an extreme
+        mn[d] = fminf(mn[d], v);
+        mx[d] = fmaxf(mx[d], v);
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < DD; ++d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[d] = fminf(mn[d], __shfl_xor_sync(kFull, mn[d], o));
+      mx[d] = fmaxf(mx[d], __shfl_xor_sync(kFull, mx[d], o));
+    }
+    if (lane == 0) {
+      red[2 * d][warp] = mn[d];
+      red[2 * d + 1][warp] = mx[d];
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const bool in = lane < (int)(blockDim.x >> 5);
+#pragma unroll
+    for (int d = 0; d < DD; ++d) {
+      float lo = in ? red[2 * d][lane] : FLT_MAX, hi = in ? red[2 * d + 1][lane] : -FLT_MAX;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(kFull, hi, o));
+      }
+      if (lane == 0) {
+        atomicMin(&grid_minmax[2 * (g * kMaxDim + d)], f2ord(lo));
+        atomicMax(&grid_minmax[2 * (g * kMaxDim + d) + 1], f2ord(hi));
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_minmax(int D, CoordPtrs x, const Chunk* chunks,
                                                      const EventDesc* events, int32_t* grid_minmax) {
   __shared__ float red[32];
   const Chunk c = chunks[blockIdx.x];
   const int g = events[c.event].grid;
+  if (D == 2)
+    return minmax_fixed<2>(x, c, g, grid_minmax);
+  if (D == 3)
+    return minmax_fixed<3>(x, c, g, grid_minmax);
   for (int d = 0; d < D; ++d) {
     float mn = FLT_MAX, mx = -FLT_MAX;
     for (int i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
