@@ -297,6 +297,26 @@ def test_sample_associations_full_csr_mixed_batch():
         assert np.array_equal(offsets, expected_sample_offsets(o, len(sizes)))
 
 
+@pytest.mark.parametrize("ordered_events", ["half", "one"])
+def test_batch_mixing_exact_and_ordered_sums(ordered_events):
+    # Events whose sums are exact in any order (unit weights) beside events
+    # whose sums keep the reference's order (exponential weights): the tile
+    # sort must still order the tiles of the latter, with counting-sort
+    # binning, whether half the events or a single one need it.
+    ev, sizes = W.batch_2d(32, 256, 8192, seed=41)
+    offs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64))])
+    w = np.ones(ev.n, np.float32)
+    rng = np.random.default_rng(42)
+    pick = range(0, len(sizes), 2) if ordered_events == "half" else [len(sizes) // 2]
+    for e in pick:
+        w[offs[e]:offs[e + 1]] = rng.exponential(1.0, int(sizes[e])).astype(np.float32)
+    for mode in (clue.GRID_PER_EVENT, clue.GRID_SHARED):
+        c = clue.Clusterer(1.5, 5.0, 1.5)
+        c.set_tuning(tile_binning=0)
+        for path in ("host", "device"):
+            check(ev.coords, w, 1.5, 5.0, 1.5, sizes=sizes, grid_mode=mode, path=path, clusterer=c)
+
+
 def with_empty_events(sizes, where):
     """`sizes` with a batch item of size 0 inserted before each position in
     `where` (len(sizes) appends one at the end)."""
