@@ -50,17 +50,17 @@ CONFIG = {
 # index and writes nh (4D + 12); the whole pipeline moves 20D + 64.
 BYTES_PER_POINT = {"density": lambda D: 4 * D + 8, "nearest_higher": lambda D: 4 * D + 12,
                    "pipeline": lambda D: 20 * D + 64}
-# DRAM bytes (read + write) per point of each sweep, from one ncu capture of
-# the 1,024-event batch (10,621,973 points): 920.0 MB for the density sweep,
-# 733.4 MB for the nearest-higher search; a launch's traffic grows with the
-# points it processes.
-DRAM_BYTES_PER_POINT = {"density": 86.6, "nearest_higher": 69.0}
+# DRAM bytes (read + write) per point of each sweep, from one ncu capture
+# (--set full) of the 1,024-event batch (10,621,973 points): 922.2 MB for the
+# density sweep, 738.3 MB for the nearest-higher search; a launch's traffic
+# grows with the points it processes.
+DRAM_BYTES_PER_POINT = {"density": 86.8, "nearest_higher": 69.5}
 # Warp instructions per point of each sweep (smsp__inst_executed.sum / points),
-# from the same capture: 2.648 G for density, 1.609 G for nearest higher. The
+# from the same capture: 2.653 G for density, 1.609 G for nearest higher. The
 # sweeps are bound by instruction issue: the issue roofline is SMs x 4
 # schedulers x one warp instruction per cycle at the SM clock sampled during
 # the timed steps.
-INST_PER_POINT = {"density": 249.3, "nearest_higher": 151.5}
+INST_PER_POINT = {"density": 249.8, "nearest_higher": 151.5}
 
 
 def measured_peaks():
